@@ -1,0 +1,643 @@
+/*
+ * felog_oracle.c - CPU restatement of FeLoG's graph-embedding hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY (see felog_oracle.h).  Plain C, single-threaded,
+ * written for small cases.  Floating-point expressions keep the reference's
+ * operation order; a*b+c is not contracted (built with -ffp-contract=off)
+ * except where the reference's CUDA kernels fuse it, which is written out
+ * with fmaf().
+ */
+#include "felog_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+/* ------------------------------------------------------------------ CSR */
+
+/* graph.hpp:741-772 (undirected doubling, e then its transpose),
+ * graph.hpp:781-785 (out-degree), graph.hpp:531-575 (bucket by src in order). */
+int orc_build_csr(const orc_edge12 *edges, uint64_t n, uint32_t v_num, int undirected, orc_csr *out) {
+  uint64_t m = undirected ? 2 * n : n;
+  memset(out, 0, sizeof(*out));
+  out->v_num = v_num;
+  out->e_num = m;
+  out->row_ptr = (uint64_t *)calloc((size_t)v_num + 1, sizeof(uint64_t));
+  out->nbr = (uint32_t *)malloc((m ? m : 1) * sizeof(uint32_t));
+  out->data = (float *)malloc((m ? m : 1) * sizeof(float));
+  uint64_t *fill = (uint64_t *)calloc((size_t)v_num + 1, sizeof(uint64_t));
+  if (!out->row_ptr || !out->nbr || !out->data || !fill) return -1;
+  for (uint64_t i = 0; i < m; i++) {
+    const orc_edge12 *e = &edges[undirected ? i / 2 : i];
+    uint32_t src = (undirected && (i & 1)) ? e->dst : e->src;
+    if (src >= v_num) { free(fill); return -2; }
+    out->row_ptr[src + 1]++;
+  }
+  for (uint32_t v = 0; v < v_num; v++) out->row_ptr[v + 1] += out->row_ptr[v];
+  for (uint32_t v = 0; v < v_num; v++) fill[v] = out->row_ptr[v];
+  for (uint64_t i = 0; i < m; i++) {
+    const orc_edge12 *e = &edges[undirected ? i / 2 : i];
+    int t = undirected && (i & 1);
+    uint32_t src = t ? e->dst : e->src, dst = t ? e->src : e->dst;
+    uint64_t pos = fill[src]++;
+    out->nbr[pos] = dst;
+    out->data[pos] = e->data;
+  }
+  free(fill);
+  return 0;
+}
+
+void orc_free_csr(orc_csr *c) {
+  free(c->row_ptr);
+  free(c->nbr);
+  free(c->data);
+  memset(c, 0, sizeof(*c));
+}
+
+/* ---------------------------------------------------------- Correlation */
+
+/* SetProperty(0,1,0,1,0,0,1,1,1) at the first visit, walk.hpp:928-933 */
+void orc_corr_init(orc_corr *c) {
+  c->Hn = 0.0; c->Sn = 1.0; c->EnH = 0.0; c->EnS = 1.0; c->EnHS = 0.0;
+  c->EnHH = 0.0; c->EnSS = 1.0; c->N = 1.0; c->R = 1.0;
+}
+
+/* Correlation::iterate with step_k = 1, walk.hpp:296-366 */
+void orc_corr_iterate(orc_corr *c, double fi) {
+  const double step_k = 1.0;
+  double Sn = c->Sn, Hn = c->Hn;
+  /* SnSn_div_Snp1Snp1, walk.hpp:296-301 */
+  double Snp1a = Sn + step_k;
+  double ss = pow(Sn / Snp1a, Sn) * pow(1.0 / Snp1a, step_k);
+  double t;
+  if (fi == 0.0) {
+    t = log2(ss);
+  } else {
+    /* FjFj_div_FiFi, walk.hpp:303-307 */
+    double fj = fi + step_k;
+    double ff = pow(fj / fi, fi) * pow(fj, step_k);
+    t = log2(ss * ff);
+  }
+  double Hnp1 = (Sn * Hn - t) / (Sn + step_k); /* walk.hpp:314 */
+  double Snp1 = c->Sn + step_k;
+  double Np1 = c->N + 1.0;
+  double EH = c->EnH + (Hnp1 - c->EnH) / Np1; /* iterateEX, walk.hpp:322-324 */
+  double ES = c->EnS + (Snp1 - c->EnS) / Np1;
+  double EHS = c->EnHS + (Hnp1 * Snp1 - c->EnHS) / Np1;
+  double EHH = c->EnHH + (Hnp1 * Hnp1 - c->EnHH) / Np1;
+  double ESS = c->EnSS + (Snp1 * Snp1 - c->EnSS) / Np1;
+  double DH = EHH - EH * EH;
+  double DS = ESS - ES * ES;
+  double ex = EHS - EH * ES;
+  c->R = ex == 0.0 ? 0.0 : ex / sqrt(DH * DS);
+  c->Hn = Hnp1; c->Sn = Snp1; c->EnH = EH; c->EnS = ES; c->EnHS = EHS;
+  c->EnHH = EHH; c->EnSS = ESS; c->N = Np1;
+}
+
+/* walk.hpp:945-951, :1056-1062: stop once step > minLength and R^2 < 0.999 or R < 0 */
+int orc_corr_stop(const orc_corr *c, uint32_t step, uint32_t min_len) {
+  if (step > min_len) {
+    if (pow(c->R, 2) < 0.999 || c->R < 0) return 1;
+  }
+  return 0;
+}
+
+/* ---------------------------------------------------------------- RNG */
+
+void orc_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]) {
+  uint32_t c0 = ctr[0], c1 = ctr[1], c2 = ctr[2], c3 = ctr[3];
+  uint32_t k0 = key[0], k1 = key[1];
+  for (int r = 0; r < 10; r++) {
+    uint64_t p0 = (uint64_t)0xD2511F53u * c0;
+    uint64_t p1 = (uint64_t)0xCD9E8D57u * c2;
+    uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+    uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+    uint32_t n0 = hi1 ^ c1 ^ k0, n1 = lo1, n2 = hi0 ^ c3 ^ k1, n3 = lo0;
+    c0 = n0; c1 = n1; c2 = n2; c3 = n3;
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+  }
+  out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
+}
+
+static inline uint32_t mulhi64_u32(uint64_t r, uint32_t n) {
+  return (uint32_t)(((unsigned __int128)r * n) >> 64);
+}
+
+void orc_walk_draw(uint64_t seed, uint32_t start, uint32_t round, uint32_t iter, uint32_t replica,
+                   uint32_t deg, uint32_t *index, double *p) {
+  uint32_t ctr[4] = {start, round, iter, replica};
+  uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+  uint32_t o[4];
+  orc_philox4x32_10(ctr, key, o);
+  *index = mulhi64_u32(((uint64_t)o[3] << 32) | o[0], deg);
+  *p = (double)((((uint64_t)o[1] << 32) | o[2]) >> 11) * (1.0 / 9007199254740992.0);
+}
+
+/* --------------------------------------------------------------- walk */
+
+static uint64_t count_in(const uint32_t *path, uint64_t n, uint32_t v) {
+  uint64_t c = 0;
+  for (uint64_t i = 0; i < n; i++) c += path[i] == v;
+  return c;
+}
+
+int orc_walk_round(const orc_csr *g, uint32_t walker_num, const uint8_t *stop_flags, uint32_t min_len,
+                   uint64_t seed, uint32_t round, const orc_draws *inj, uint32_t *tokens,
+                   uint64_t tok_cap, uint64_t *sent_off, uint32_t *sent_walker, orc_walk_stats *st) {
+  const uint32_t V = g->v_num;
+  memset(st, 0, sizeof(*st));
+  uint64_t ntok = 0, k = 0;
+  sent_off[0] = 0;
+  for (uint32_t w = 0; w < walker_num; w++) {
+    uint32_t start = w % V; /* walk.hpp:519-527 */
+    if (stop_flags && stop_flags[start]) continue; /* walk.hpp:570 */
+    uint32_t replica = w / V;
+    uint64_t di = 0, dp = 0; /* consumed injected draws */
+    uint32_t iter = 0;
+    uint32_t *path = tokens + ntok;
+    uint64_t len = 0;
+    if (ntok + 1 > tok_cap) return -1;
+    path[len++] = start; /* step-0 footprint, walk.hpp:691-699 */
+    orc_corr c;
+    orc_corr_init(&c); /* first visit: fi = 0 consumed, walk.hpp:926-933 */
+    uint32_t cur = start, step = 0;
+    for (;;) {
+      uint64_t b = g->row_ptr[cur];
+      uint32_t deg = (uint32_t)(g->row_ptr[cur + 1] - b);
+      if (deg == 0) break; /* walk.hpp:964-969 */
+      uint32_t r;
+      double p = 0.0;
+      if (inj) {
+        if (inj->idx_off[k] + di >= inj->idx_off[k + 1]) return -2;
+        r = inj->idx[inj->idx_off[k] + di++];
+      } else {
+        orc_walk_draw(seed, start, round, iter, replica, deg, &r, &p);
+      }
+      iter++;
+      st->n_iterations++;
+      if (deg == 2 && g->nbr[b] == cur) break;               /* walk.hpp:977-979 */
+      uint64_t cand = b + r;
+      if (step == 0 && g->nbr[cand] == cur) continue;        /* walk.hpp:981-983 */
+      int cn = (int)g->data[cand];                          /* walk.hpp:997 */
+      if (inj) {
+        if (inj->p_off[k] + dp >= inj->p_off[k + 1]) return -2;
+        p = inj->p[inj->p_off[k] + dp++];
+      }
+      int sd = (int)deg;
+      uint32_t dst = g->nbr[cand];
+      int dd = (int)(g->row_ptr[dst + 1] - g->row_ptr[dst]);
+      int mx = sd > dd ? sd : dd, mn = sd < dd ? sd : dd;
+      double p_accept = (1 / ((double)(sd - cn)) * ((double)mx) / mn); /* walk.hpp:1010 */
+      double p_norm = tanh(p_accept);
+      int trace = p_norm <= p;                                        /* walk.hpp:1015 */
+      st->n_traces += trace;
+      step++;
+      if (ntok + len + 1 > tok_cap) return -1;
+      path[len++] = dst;                                              /* walk.hpp:1038-1041 */
+      orc_corr_iterate(&c, (double)count_in(path, len - 1, dst));
+      if (orc_corr_stop(&c, step, min_len)) break;
+      if (trace) {                                                    /* walk.hpp:1063-1094 */
+        step++;
+        if (ntok + len + 1 > tok_cap) return -1;
+        path[len++] = cur;
+        orc_corr_iterate(&c, (double)count_in(path, len - 1, cur));
+        if (orc_corr_stop(&c, step, min_len)) break;
+      } else {
+        cur = dst;
+      }
+    }
+    ntok += len;
+    if (len > 64) st->n_long++;
+    sent_off[k + 1] = ntok;
+    if (sent_walker) sent_walker[k] = w;
+    k++;
+  }
+  st->n_sentences = k;
+  st->n_tokens = ntok;
+  return 0;
+}
+
+/* walk.hpp:754-787 */
+double orc_round_kl(const uint32_t *deg, const uint64_t *freq, uint32_t v_num) {
+  uint64_t words_sum = 0, degree_sum = 0;
+  for (uint32_t i = 0; i < v_num; i++) {
+    words_sum += freq[i];
+    degree_sum += deg[i];
+  }
+  double h = 0.0;
+  for (uint32_t i = 0; i < v_num; i++) {
+    double pi = (double)deg[i] / degree_sum;
+    double qi = (double)freq[i] / words_sum;
+    h += pi * (log(pi) - log(qi));
+  }
+  return h;
+}
+
+float orc_lr(float initial, float decay, int r) { return initial * expf(-decay * r); }
+
+/* ------------------------------------------------------------ trainer */
+
+typedef struct {
+  long long cn;
+  uint32_t v;
+} vw;
+
+static int vw_cmp(const void *a, const void *b) {
+  const vw *x = (const vw *)a, *y = (const vw *)b;
+  if (x->cn != y->cn) return x->cn < y->cn ? 1 : -1;
+  return x->v < y->v ? -1 : (x->v > y->v ? 1 : 0); /* stable: keeps id order */
+}
+
+int orc_vocab(const uint32_t *deg, uint32_t v_num, long long min_count, uint32_t *vocab_vertex,
+              long long *vocab_cn, uint32_t *id2offset, long long *vocab_size, long long *train_words) {
+  vw *a = (vw *)malloc(sizeof(vw) * (v_num ? v_num : 1));
+  if (!a) return -1;
+  for (uint32_t v = 0; v < v_num; v++) {
+    a[v].cn = deg[v];
+    a[v].v = v;
+  }
+  qsort(a, v_num, sizeof(vw), vw_cmp);
+  long long size = v_num, tw = 0;
+  for (uint32_t i = 0; i < v_num; i++) { /* SortVocab, word2vec.cu:740-748 */
+    if (a[i].cn < min_count && i != 0) size--;
+    else tw += a[i].cn;
+  }
+  for (uint32_t v = 0; v < v_num; v++) id2offset[v] = 0xFFFFFFFFu;
+  for (long long i = 0; i < size; i++) {
+    vocab_vertex[i] = a[i].v;
+    vocab_cn[i] = a[i].cn;
+    id2offset[a[i].v] = (uint32_t)i;
+  }
+  *vocab_size = size;
+  *train_words = tw;
+  free(a);
+  return 0;
+}
+
+void orc_unigram_table(const long long *cn, long long vocab_size, int32_t *table, int64_t table_size) {
+  double train_words_pow = 0, d1, power = 0.75;
+  long long a, i;
+  for (a = 0; a < vocab_size; a++) train_words_pow += pow((double)cn[a], power);
+  i = 0;
+  d1 = pow((double)cn[i], power) / train_words_pow;
+  for (a = 0; a < table_size; a++) {
+    table[a] = (int32_t)i;
+    if (a / (double)table_size > d1) {
+      i++;
+      d1 += pow((double)cn[i < vocab_size ? i : vocab_size - 1], power) / train_words_pow;
+    }
+    if (i >= vocab_size) i = vocab_size - 1;
+  }
+}
+
+int orc_subsample_thresholds(const long long *cn, long long vocab_size, double sample,
+                             long long train_words, uint16_t *thr) {
+  if (sample <= 0.0 || train_words <= 0) return 0;
+  const double stw = sample * (double)train_words;
+  if (stw <= 0.0 || vocab_size <= 0) return 0;
+  for (long long i = 0; i < vocab_size; i++) {
+    long long count = cn[i];
+    if (count <= 0) {
+      thr[i] = 65535;
+      continue;
+    }
+    double prob = (sqrt(count / stw) + 1.0) * (stw / (double)count);
+    if (prob > 1.0) prob = 1.0;
+    else if (prob < 0.0) prob = 0.0;
+    thr[i] = prob >= 1.0 ? 65535 : (uint16_t)(prob * 65535.0 + 0.5);
+  }
+  return 1;
+}
+
+void orc_exp_table(float *t) {
+  for (int i = 0; i < 1000; i++) {
+    t[i] = expf((i / (float)1000 * 2 - 1) * 6);
+    t[i] = t[i] / (t[i] + 1);
+  }
+}
+
+/* FastRandomState, word2vec.cu:134-152 */
+typedef struct {
+  unsigned long long state;
+} fast_rng;
+static uint32_t rng_next32(fast_rng *r) {
+  r->state = r->state * 25214903917ULL + 11ULL;
+  return (uint32_t)(r->state >> 16);
+}
+
+int orc_plan_batches(const uint32_t *tokens, const uint64_t *sent_off, uint64_t n_corpus_sent,
+                     const uint32_t *id2offset, const uint16_t *thr, int use_thr, const int32_t *table,
+                     int64_t table_size, long long vocab_size, int negative, int rank, orc_plan_out *out) {
+  fast_rng rng;
+  unsigned long long seed = 0x9E3779B97F4A7C15ULL ^ (((unsigned long long)rank + 1ULL) << 1) ^ 0x2ULL;
+  rng.state = seed ? seed : 1ULL;
+  uint64_t ci = 0, total = 0, s_out = 0, nb = 0;
+  long long word = 0;
+  out->words_considered = 0;
+  out->sent_start[0] = 0;
+  while (ci < n_corpus_sent) {
+    uint64_t batch_base = total;
+    int cnt = 0;
+    out->batch_first[nb] = s_out;
+    while (cnt < 15000 && ci < n_corpus_sent) { /* word2vec.cu:1193-1235 */
+      int temp = 0;
+      for (uint64_t t = sent_off[ci]; t < sent_off[ci + 1]; t++) {
+        uint32_t off = id2offset[tokens[t]];
+        if (off == 0xFFFFFFFFu) continue; /* out of vocabulary */
+        word = (long long)off;
+        out->words_considered++;
+        if (word == 0) break;
+        if (use_thr) {
+          uint16_t keep = thr[word];
+          if (keep < 65535) {
+            uint16_t r16 = (uint16_t)(rng_next32(&rng) >> 16);
+            if (r16 > keep) continue;
+          }
+        }
+        if (total >= out->sen_cap) return -1;
+        out->sen[total++] = (int32_t)word;
+        temp++;
+        if (temp >= 1000) break;
+      }
+      cnt++;
+      s_out++;
+      out->sent_start[s_out] = total;
+      ci++;
+      if (total - batch_base >= (uint64_t)(15000 - 1) * 20) break;
+    }
+    if (cnt == 0) break;
+    for (int i = 0; i < cnt * negative; i++) { /* word2vec.cu:1240-1248 */
+      uint32_t randd = rng_next32(&rng);
+      int32_t ts = table[randd % (uint64_t)table_size];
+      out->negs[(out->batch_first[nb]) * negative + i] =
+          ts == 0 ? (int32_t)(randd % (uint64_t)(vocab_size - 1)) + 1 : ts;
+    }
+    nb++;
+  }
+  out->batch_first[nb] = s_out;
+  out->n_sentences = s_out;
+  out->n_batches = nb;
+  out->n_sen = total;
+  return (int)s_out;
+}
+
+/* dot product in skip_gram_kernel's order (FSIZE = dim / 2, word2vec.cu:510-518) */
+static float sg_dot(const float *x, const float *y, int dim) {
+  int fs = dim / 2;
+  float f[512];
+  for (int t = 0; t < fs; t++) f[t] = x[t] * y[t];
+  for (int t = fs; t < dim; t++) f[t % fs] = fmaf(x[t], y[t], f[t % fs]);
+  for (int i = fs / 2; i > 0; i /= 2)
+    for (int t = 0; t < i; t++) f[t] += f[i + t];
+  return f[0];
+}
+
+static float sg_gradient(float f, int label, const float *exp_table, float alpha) {
+  if (f > 6) return (label - 1) * alpha;
+  if (f < -6) return (label - 0) * alpha;
+  return (label - exp_table[(int)((f + 6) * (1000 / 6 / 2))]) * alpha;
+}
+
+void orc_skipgram_batch(float *syn0, float *syn1, const float *exp_table, const int32_t *table,
+                        int64_t table_size, long long vocab_size, const int32_t *sen,
+                        const uint64_t *sent_start, uint64_t first_sentence, uint64_t n_sentences,
+                        int window, int dim, int negative, float alpha) {
+  float neu1e[512];
+  for (uint64_t blk = 0; blk < n_sentences; blk++) {
+    uint64_t s = first_sentence + blk;
+    long long sidx_s = (long long)sent_start[s], sidx_e = (long long)sent_start[s + 1];
+    unsigned long next_random = (unsigned long)blk; /* blockIdx.x within the batch */
+    for (long long pos = sidx_s; pos < sidx_e; pos++) {
+      int word = sen[pos];
+      if (word == -1) continue;
+      next_random = next_random * (unsigned long)2514903917 + 11;
+      int b = (int)(next_random % (unsigned long)window);
+      for (int a = b; a < window * 2 + 1 - b; a++) {
+        if (a == window) continue;
+        long long c = pos - window + a;
+        if (c < sidx_s || c >= sidx_e) continue;
+        int last_word = sen[c];
+        if (last_word == -1) continue;
+        float *x = syn0 + (long long)last_word * dim;
+        for (int t = 0; t < dim; t++) neu1e[t] = 0;
+        for (int d = 0; d < negative + 1; d++) {
+          int target, label;
+          if (d == 0) {
+            target = word;
+            label = 1;
+          } else {
+            next_random = next_random * (unsigned long)25214903917 + 11;
+            target = table[(next_random >> 16) % (unsigned long)table_size];
+            if (target == 0) target = (int)(next_random % (unsigned long)(vocab_size - 1) + 1);
+            if (target == word) continue;
+            label = 0;
+          }
+          float *y = syn1 + (long long)target * dim;
+          float f = sg_dot(x, y, dim);
+          float g = sg_gradient(f, label, exp_table, alpha);
+          for (int t = 0; t < dim; t++) {
+            neu1e[t] = fmaf(g, y[t], neu1e[t]);
+            y[t] += g * x[t];
+          }
+        }
+        for (int t = 0; t < dim; t++) x[t] += neu1e[t];
+      }
+    }
+  }
+}
+
+/* plain sequential dot for the reuse-neg algorithm (true dot product) */
+static float seq_dot(const float *x, const float *y, int dim) {
+  float f = 0;
+  for (int t = 0; t < dim; t++) f = fmaf(x[t], y[t], f);
+  return f;
+}
+
+void orc_negreuse_batch(float *syn0, float *syn1, const float *exp_table, const int32_t *sen,
+                        const uint64_t *sent_start, uint64_t first_sentence, uint64_t n_sentences,
+                        const int32_t *negs, int window, int dim, int negative, float alpha) {
+  float neu1e[512];
+  float g[64];
+  int tgt[64];
+  for (uint64_t blk = 0; blk < n_sentences; blk++) {
+    uint64_t s = first_sentence + blk;
+    long long ss = (long long)sent_start[s], se = (long long)sent_start[s + 1];
+    const int32_t *neg = negs + s * (uint64_t)negative;
+    for (long long pos = ss; pos < se; pos++) {
+      int word = sen[pos];
+      if (word == -1) continue;
+      for (int a = 0; a < window * 2 + 1; a++) {
+        if (a == window) continue;
+        long long c = pos - window + a;
+        if (c < ss || c >= se || sen[c] == -1) continue;
+        float *x = syn0 + (long long)sen[c] * dim;
+        int nt = 0;
+        for (int y = 0; y <= negative; y++) { /* warp y < K: negative y, warp K: positive */
+          int target = y == negative ? word : neg[y];
+          if (y < negative && target == word) continue;
+          int label = y == negative ? 1 : 0;
+          float f = seq_dot(x, syn1 + (long long)target * dim, dim);
+          g[nt] = sg_gradient(f, label, exp_table, alpha);
+          tgt[nt++] = target;
+        }
+        for (int t = 0; t < dim; t++) neu1e[t] = 0;
+        for (int k = 0; k < nt; k++) {
+          float *yv = syn1 + (long long)tgt[k] * dim;
+          for (int t = 0; t < dim; t++) neu1e[t] = fmaf(g[k], yv[t], neu1e[t]);
+        }
+        for (int k = 0; k < nt; k++) {
+          float *yv = syn1 + (long long)tgt[k] * dim;
+          for (int t = 0; t < dim; t++) yv[t] += g[k] * x[t];
+        }
+        for (int t = 0; t < dim; t++) x[t] += neu1e[t];
+      }
+    }
+  }
+}
+
+void orc_cbow_batch(float *syn0, float *syn1, const float *exp_table, const int32_t *table,
+                    int64_t table_size, long long vocab_size, const int32_t *sen,
+                    const uint64_t *sent_start, uint64_t first_sentence, uint64_t n_sentences,
+                    int window, int dim, int negative, float alpha) {
+  float neu1[512], neu1e[512];
+  for (uint64_t blk = 0; blk < n_sentences; blk++) {
+    uint64_t s = first_sentence + blk;
+    long long ss = (long long)sent_start[s], se = (long long)sent_start[s + 1];
+    unsigned long next_random = (unsigned long)blk;
+    for (long long pos = ss; pos < se; pos++) {
+      int word = sen[pos];
+      if (word == -1) continue;
+      for (int t = 0; t < dim; t++) neu1[t] = neu1e[t] = 0;
+      next_random = next_random * (unsigned long)2514903917 + 11;
+      int b = (int)(next_random % (unsigned long)window);
+      int cw = 0;
+      for (int a = b; a < window * 2 + 1 - b; a++) {
+        if (a == window) continue;
+        long long c = pos - window + a;
+        if (c < ss || c >= se || sen[c] == -1) continue;
+        const float *x = syn0 + (long long)sen[c] * dim;
+        for (int t = 0; t < dim; t++) neu1[t] += x[t];
+        cw++;
+      }
+      if (!cw) continue;
+      for (int t = 0; t < dim; t++) neu1[t] /= cw;
+      for (int d = 0; d < negative + 1; d++) {
+        int target, label;
+        if (d == 0) {
+          target = word;
+          label = 1;
+        } else {
+          next_random = next_random * (unsigned long)25214903917 + 11;
+          target = table[(next_random >> 16) % (unsigned long)table_size];
+          if (target == 0) target = (int)(next_random % (unsigned long)(vocab_size - 1) + 1);
+          if (target == word) continue;
+          label = 0;
+        }
+        float *y = syn1 + (long long)target * dim;
+        float f = sg_dot(neu1, y, dim);
+        float g = sg_gradient(f, label, exp_table, alpha);
+        for (int t = 0; t < dim; t++) {
+          neu1e[t] = fmaf(g, y[t], neu1e[t]);
+          y[t] += g * neu1[t];
+        }
+      }
+      for (int a = b; a < window * 2 + 1 - b; a++) {
+        if (a == window) continue;
+        long long c = pos - window + a;
+        if (c < ss || c >= se || sen[c] == -1) continue;
+        float *x = syn0 + (long long)sen[c] * dim;
+        for (int t = 0; t < dim; t++) x[t] += neu1e[t];
+      }
+    }
+  }
+}
+
+void orc_init_net(float *syn0, float *syn1, long long vocab_size, int dim) {
+  unsigned long long next_random = 1;
+  for (long long a = 0; a < vocab_size; a++)
+    for (int b = 0; b < dim; b++) {
+      next_random = next_random * (unsigned long long)25214903917 + 11;
+      syn0[a * dim + b] = (((next_random & 0xFFFF) / (float)65536) - 0.5) / dim;
+    }
+  if (syn1) memset(syn1, 0, sizeof(float) * (size_t)vocab_size * (size_t)dim);
+}
+
+/* batch_similarity_direct_index_optimized_kernel order with blockDim = 128 (dim <= 128) */
+float orc_cosine(const float *a, const float *b, int dim) {
+  float sd[256], sa[256], sb[256];
+  int bd = dim > 200 ? 256 : 128;
+  for (int t = 0; t < bd; t++) {
+    float x = t < dim ? a[t] : 0.0f, y = t < dim ? b[t] : 0.0f;
+    sd[t] = x * y;
+    sa[t] = x * x;
+    sb[t] = y * y;
+  }
+  for (int s = bd / 2; s > 0; s >>= 1)
+    for (int t = 0; t < s; t++) {
+      sd[t] += sd[t + s];
+      sa[t] += sa[t + s];
+      sb[t] += sb[t + s];
+    }
+  float na = sqrtf(sa[0]), nb = sqrtf(sb[0]);
+  if (na == 0.0f || nb == 0.0f) return 0.0f;
+  return sd[0] / (na * nb);
+}
+
+void orc_eval_choose(uint64_t seed, uint32_t round, uint32_t v, uint32_t deg, uint32_t *chosen) {
+  /* partial Fisher-Yates over positions 0..deg-1, first 30 positions */
+  uint32_t pos[30], val[30];
+  int nsw = 0;
+  for (uint32_t i = 0; i < 30; i++) {
+    uint32_t ctr[4] = {v, round, i, 0x45564C31u};
+    uint32_t key[2] = {(uint32_t)seed ^ 0x2545F491u, (uint32_t)(seed >> 32)};
+    uint32_t o[4];
+    orc_philox4x32_10(ctr, key, o);
+    uint32_t j = i + mulhi64_u32(((uint64_t)o[1] << 32) | o[0], deg - i);
+    /* current values at positions i and j */
+    uint32_t vi = i, vj = j;
+    int hi = -1, hj = -1;
+    for (int k = 0; k < nsw; k++) {
+      if (pos[k] == i) hi = k;
+      if (pos[k] == j) hj = k;
+    }
+    if (hi >= 0) vi = val[hi];
+    if (hj >= 0) vj = val[hj];
+    chosen[i] = vj;
+    /* position j now holds vi (position i is never read again) */
+    if (hj >= 0) val[hj] = vi;
+    else { pos[nsw] = j; val[nsw] = vi; nsw++; }
+  }
+}
+
+uint64_t orc_convergence(const float *syn0, const uint32_t *id2offset, int dim, const orc_csr *g,
+                         uint8_t *stop_flags, uint64_t seed, uint32_t round, float *sim) {
+  uint64_t eva = 0;
+  uint32_t chosen[30];
+  for (uint32_t v = 0; v < g->v_num; v++) {
+    if (stop_flags[v]) continue; /* word2vec.cu:2023-2027 */
+    uint64_t b = g->row_ptr[v];
+    uint32_t deg = (uint32_t)(g->row_ptr[v + 1] - b);
+    int n = deg;
+    if (deg > 30) {
+      n = 30;
+      orc_eval_choose(seed, round, v, deg, chosen);
+    } else {
+      for (uint32_t i = 0; i < deg; i++) chosen[i] = i;
+    }
+    float s = 0.0f;
+    if (n > 0) {
+      float sum = 0.0f;
+      const float *a = syn0 + (uint64_t)id2offset[v] * dim;
+      for (int j = 0; j < n; j++) {
+        uint32_t u = g->nbr[b + chosen[j]];
+        sum += orc_cosine(a, syn0 + (uint64_t)id2offset[u] * dim, dim);
+      }
+      s = sum / n;
+    }
+    if (sim) sim[v] = s;
+    if (s > 0.65) stop_flags[v] = 1; /* word2vec.cu:2056-2061 */
+    else eva++;
+  }
+  return eva;
+}
