@@ -1,0 +1,366 @@
+#!/usr/bin/env python
+"""Benchmark of the FeLoG graph-embedding hot path on B200.
+
+Workload (default): the plain-FP32 mid-scale configuration - a seed-1 R-MAT
+graph (a, b, c, d = .57, .19, .19, .05) over 2,238,731 vertex ids with
+34.7M unique undirected edges, float32 weights uniform in (0, 1], 5 % of the
+edges held out (isolated vertices removed), min_L 20, min_R 2, skip-gram
+dim 128 FP32, window 10, negative 5, sample 1e-3, reuse-neg 0.  Synthetic
+data (seeded); the tables and CSR are larger than L2, so no flush is needed.
+
+One step = one round of the hot path: a walk round over every vertex whose
+walkers are not stopped (biased walk + information-centric stop), the
+trainer's batch plan and skip-gram pass over that round's corpus, and the
+per-vertex convergence check (from round min_R on).  `value` is corpus
+tokens per second through the whole round (each token is one walk step and
+one trainer word), timed with CUDA events on the library's stream; `e2e` is
+the same through the C ABI with the round's stop flags copied in from pinned
+host memory and the trained embeddings copied back every round (the
+reference copies syn0 back after every round, word2vec.cu:1264).
+
+`--impl reference` times the reference's own implementation of the path
+(oracle/_ref, compiled from the reference sources) on the box: its CPU walk
+engine with all host threads and its CUDA skip-gram kernels.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "info-centric_ge_b200"))
+
+CONFIGS = {
+    "c2": dict(workload="plain FP32, seed-1 R-MAT 2,238,731 vertex ids / 34.7M undirected edges, 5% held out",
+               seed=1, v_target=2238731, e_target=34_700_000, abcd=(0.57, 0.19, 0.19, 0.05), lognormal=False,
+               holdout=0.05),
+    "c1": dict(workload="plain FP32, seed-0 R-MAT 16,384 vertex ids / 131,072 undirected edges, 10% held out",
+               seed=0, v_target=16384, e_target=131072, abcd=(0.57, 0.19, 0.19, 0.05), lognormal=False,
+               holdout=0.10),
+}
+TRAIN = dict(min_length=20, min_rounds=2, size=128, window=10, negative=5, sample=1e-3, cbow=0, reuse_neg=0,
+             min_count=0)
+METRIC = "walk+SGNS corpus tokens/s (walk steps/s and SGNS words/s reported alongside)"
+WALK_BYTES_PER_STEP = 68      # 2 random 32-B sectors + 4-B token write
+SGNS_BYTES_PER_PAIR = 7168    # 14 rows x 128 x 4 B (read + write syn0 row and 6 syn1 rows)
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi samples during the timed region (median SM clock, throttle reasons)."""
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.t.join(timeout=2)
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def make_graph(cfg):
+    import felog_b200 as fb
+    t = time.time()
+    g = fb.synth_graph(seed=cfg["seed"], v_target=cfg["v_target"], e_target=cfg["e_target"], abcd=cfg["abcd"],
+                       lognormal=cfg["lognormal"], holdout=cfg["holdout"])
+    log(f"graph: {g['info']} in {time.time() - t:.1f}s")
+    return g
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=300))
+        pg = dist
+    return world, rank, local, pg
+
+
+def max_over_ranks(pg, x):
+    if pg is None:
+        return x
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(pg, x):
+    if pg is None:
+        return x
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64)
+    pg.all_reduce(t, op=pg.ReduceOp.SUM)
+    return float(t.item())
+
+
+def run_round(f, r, min_rounds, counters):
+    ws = f.walk_round(r)
+    ts = f.train_round(r)
+    counters["tokens"] += ws["n_tokens"]
+    counters["words"] += ts["words"]
+    counters["pairs"] += ts["pairs"]
+    counters["walk_ms"] += ws["ms"]
+    counters["train_ms"] += ts["ms_train"]
+    counters["plan_ms"] += ts["ms_plan"]
+    if r + 1 >= min_rounds:
+        bs = f.budget_check(r)
+        counters["budget_ms"] += bs["ms"]
+
+
+def cpu_baseline(g, cfg):
+    """The oracle (CPU restatement) on a bounded sample of the workload: the walk
+    of 60k walkers and the skip-gram pass over their first 1500 sentences,
+    single-threaded; reported as corpus tokens/s through walk + train."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_binding as ob
+    V = g["v_num"]
+    c = ob.OracleCsr(g["edges"], V)
+    nw = min(60000, V)
+    t0 = time.perf_counter()
+    tok, off, _, st = ob.walk_round(c, nw, TRAIN["min_length"], seed=1, round_=0)
+    t_walk = time.perf_counter() - t0
+    vv, vcn, id2, vs, tw = ob.vocab(c.deg, 0)
+    thr, used = ob.subsample_thresholds(vcn, TRAIN["sample"], tw)
+    table = ob.unigram_table(vcn)
+    et = ob.exp_table()
+    syn0 = np.zeros(vs * 128, np.float32)
+    syn0[:] = (np.arange(vs * 128) % 97 - 48).astype(np.float32) / (97 * 128)
+    syn1 = np.zeros(vs * 128, np.float32)
+    ns = 1500
+    t2, o2 = tok[: int(off[ns])], off[: ns + 1]
+    pl = ob.plan_batches(t2, o2, id2, thr, used, table, vs, TRAIN["negative"])
+    t1 = time.perf_counter()
+    ob.skipgram_batch(syn0, syn1, et, table, vs, pl["sen"], pl["sent_start"], 0, len(pl["sent_start"]) - 1,
+                      TRAIN["window"], 128, TRAIN["negative"], 0.025)
+    t_train = time.perf_counter() - t1
+    walk_rate = len(tok) / t_walk
+    train_rate = int(o2[-1]) / t_train
+    value = 1.0 / (1.0 / walk_rate + 1.0 / train_rate)
+    return {"value": value, "unit": "tokens/s", "cores": 1, "kind": "port",
+            "sample": f"oracle walk of {nw} walkers ({len(tok)} tokens, {t_walk:.1f}s) + skip-gram over "
+                      f"{ns} sentences ({int(o2[-1])} tokens, {t_train:.1f}s), 1 thread",
+            "walk_steps_per_s": walk_rate, "sgns_words_per_s": train_rate}
+
+
+def bench_mine(args):
+    import felog_b200 as fb
+    world, rank, local, pg = dist_setup(args)
+    cfg = CONFIGS[args.config]
+    g = make_graph(cfg)
+    V = g["v_num"]
+    f = fb.Felog(v_num=V, device=local, seed=1000 + rank, **TRAIN)
+    f.load_graph(g["edges"], V)
+    f.init_model()
+    min_r = TRAIN["min_rounds"]
+    warm = {k: 0.0 for k in ("tokens", "words", "pairs", "walk_ms", "train_ms", "plan_ms", "budget_ms")}
+    for r in range(args.warmup):
+        run_round(f, r, min_r, warm)
+    log(f"warmup done: {warm}")
+    # ---- device-timed region: inputs resident in HBM
+    if pg is not None:
+        pg.barrier()
+    cnt = {k: 0.0 for k in warm}
+    launches0 = f.kernel_launches()
+    with ClockSampler(local) as clk:
+        f.timer_mark(0)
+        for r in range(args.warmup, args.warmup + args.steps):
+            run_round(f, r, min_r, cnt)
+        f.timer_mark(1)
+        ms = f.timer_elapsed()
+    launches = f.kernel_launches() - launches0
+    ms_max = max_over_ranks(pg, ms)
+    tokens_all = sum_over_ranks(pg, cnt["tokens"])
+    value = tokens_all / (ms_max * 1e-3)
+    # ---- end to end through the C ABI with host buffers
+    import ctypes
+
+    import torch
+    flags_h = torch.zeros(V, dtype=torch.uint8).pin_memory()
+    flags_h.numpy()[:] = f.stop_flags()
+    vs = f.vocab()[2]
+    emb_h = torch.empty(vs * 128, dtype=torch.float32).pin_memory()
+    e2e = {k: 0.0 for k in warm}
+    if pg is not None:
+        pg.barrier()
+    f.timer_mark(0)
+    r0 = args.warmup + args.steps
+    for r in range(r0, r0 + args.steps):
+        f.set_stop_flags_from(ctypes.c_void_p(flags_h.data_ptr()))
+        run_round(f, r, min_r, e2e)
+        f.embeddings_into(ctypes.c_void_p(emb_h.data_ptr()), vs * 128)
+        flags_h.numpy()[:] = f.stop_flags()
+    f.timer_mark(1)
+    e2e_ms = max_over_ranks(pg, f.timer_elapsed())
+    e2e_value = sum_over_ranks(pg, e2e["tokens"]) / (e2e_ms * 1e-3)
+    peak, peak_kind = measured_peaks()
+    # dominant kernel: the skip-gram pass
+    sg_achieved = cnt["pairs"] * SGNS_BYTES_PER_PAIR / (cnt["train_ms"] * 1e-3) / 1e9
+    walk_achieved = cnt["tokens"] * WALK_BYTES_PER_STEP / (cnt["walk_ms"] * 1e-3) / 1e9
+    out = {
+        "metric": METRIC,
+        "value": value,
+        "unit": "tokens/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms_max / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32 tables, f64 walk statistics",
+        "data": "synthetic (seeded R-MAT, see config)",
+        "config": {"workload": cfg["workload"], "v_num": V, "train_edges": int(len(g["edges"])),
+                   "dim": 128, "window": 10, "negative": 5, "sample": 1e-3, "min_L": 20, "min_R": 2,
+                   "skip_gram": True, "reuse_neg": 0, "l2": "inputs larger than L2 (CSR + tables > 126 MB)",
+                   "parallelism": f"replicas x{world}"},
+        "walk_steps_per_s": cnt["tokens"] / (cnt["walk_ms"] * 1e-3),
+        "sgns_words_per_s": cnt["words"] / ((cnt["train_ms"] + cnt["plan_ms"]) * 1e-3),
+        "phase_ms_per_step": {k: cnt[k] / args.steps for k in ("walk_ms", "plan_ms", "train_ms", "budget_ms")},
+        "tokens_per_step": cnt["tokens"] / args.steps,
+        "pairs_per_step": cnt["pairs"] / args.steps,
+        "roofline": {"kernel": "k_sgns_skipgram<128>", "bound": "hbm", "achieved": sg_achieved, "peak": peak,
+                     "unit": "GB/s", "frac": sg_achieved / peak, "traffic": None,
+                     "peak_source": peak_kind,
+                     "walk_kernel": {"achieved": walk_achieved, "frac": walk_achieved / peak,
+                                     "bytes_per_step": WALK_BYTES_PER_STEP}},
+        "e2e": {"value": e2e_value, "unit": "tokens/s", "h2d_bytes_per_step": int(V),
+                "d2h_bytes_per_step": int(vs * 128 * 4 + V)},
+        "gpu_launches": int(launches),
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            out["cpu_baseline"] = cpu_baseline(g, cfg)
+        except Exception as ex:  # reported, not fatal
+            out["cpu_baseline"] = {"error": str(ex)}
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    f.close()
+    if pg is not None:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+def bench_reference(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    exe = os.path.join(ROOT, "oracle", "_ref", "ref_pipeline")
+    if not os.path.exists(exe):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_pipeline was not built"}))
+        return
+    cfg = CONFIGS[args.config]
+    g = make_graph(cfg)
+    import tempfile
+    with tempfile.TemporaryDirectory() as td:
+        gp = os.path.join(td, "g.bin")
+        g["edges"].tofile(gp)
+        cmd = [exe, gp, str(g["v_num"]), str(args.warmup), str(args.steps), str(args.ref_walkers)]
+        log("reference:", " ".join(cmd))
+        res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        print(json.dumps({"impl": "reference", "unavailable": f"ref_pipeline exited {res.returncode}: "
+                                                              f"{res.stderr.strip()[-200:]}"}))
+        return
+    d = json.loads(res.stdout.strip().splitlines()[-1])
+    value = d["tokens"] / d["seconds"]
+    out = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "tokens/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": d["seconds"] * 1e3 / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded R-MAT, see config)",
+        "config": {"workload": cfg["workload"], "v_num": g["v_num"], "walkers_per_step": d["walkers"]},
+        "walk_steps_per_s": d["walk_tokens"] / d["walk_seconds"],
+        "sgns_words_per_s": d["train_words"] / d["train_seconds"],
+        "cpu_baseline": {"value": value, "unit": "tokens/s", "cores": d["threads"], "kind": "reference",
+                         "sample": f"{d['walkers']} walkers per round, {args.steps} rounds; reference walk "
+                                   f"engine on {d['threads']} host threads + reference skip_gram_kernel"},
+        "e2e": {"value": value, "unit": "tokens/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
+    ap.add_argument("--config", default="c2", choices=sorted(CONFIGS))
+    ap.add_argument("--ref-walkers", type=int, default=200000)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        bench_reference(args)
+    else:
+        bench_mine(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,231 @@
+/*
+ * felog_gpu.h - C ABI of the B200 implementation of FeLoG's graph-embedding
+ * hot path: biased random walk with the information-centric stop rule,
+ * per-vertex convergence (walk-budget) check, and skip-gram negative-sampling
+ * training.  One context owns one GPU's state: the CSR, alias tables, walk
+ * corpus, vocabulary, unigram table and embedding tables all stay resident in
+ * device memory.  Plain pointers and sizes only; the library allocates device
+ * memory, the caller owns every host buffer.  Every call returns a
+ * felog_status; felog_last_error() gives the message of the last failure.
+ * One context per host thread; all work of a context runs on its own stream.
+ *
+ * Reference seams each entry point replaces (RocmFang/Info-centric_GE paths):
+ *   felog_load_graph        GraphEngine::load_graph, include/graph.hpp:712-919
+ *   felog_build_alias       AliasTableContainer (declared, never built),
+ *                           include/walk.hpp:87-103
+ *   felog_walk_round        one round of WalkEngine::random_walk,
+ *                           include/walk.hpp:547-610, :629-752, :847-1122
+ *   felog_get_corpus        PathSet::dump -> corpus_t, include/path.hpp:70-109
+ *   felog_init_model        ReadVocabFromDegree + InitNet + InitUnigramTable,
+ *                           src/word2vec.cu:834-862, :864-902, :674-694
+ *   felog_train_round       TrainModelThreadMemory + skip_gram_kernel /
+ *                           __sgNegReuse / cbow_kernel, src/word2vec.cu:1133-1273,
+ *                           :368-646
+ *   felog_budget_check      the evaluation step of TrainModel,
+ *                           src/word2vec.cu:2016-2080, :1748-1889, :1448-1506
+ *   felog_run               the walk/train round loop of felog main +
+ *                           train_corpus_cuda, src/examples/felog.cpp:33-172,
+ *                           src/word2vec.cu:1922-2180
+ *   felog_write_embeddings  the -emb_output writer, src/word2vec.cu:2112-2127
+ */
+#ifndef FELOG_GPU_H
+#define FELOG_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FELOG_ABI_VERSION 1
+
+typedef enum felog_status {
+  FELOG_OK = 0,
+  FELOG_INVALID_ARG = 1,
+  FELOG_OOM = 2,
+  FELOG_CUDA_ERROR = 3,
+  FELOG_DEVICE_TIMEOUT = 4,
+  FELOG_INTERNAL = 5,
+  FELOG_IO_ERROR = 6,
+  FELOG_NOT_READY = 7
+} felog_status;
+
+#ifndef FELOG_EDGE12_DEFINED
+#define FELOG_EDGE12_DEFINED
+/* One binary edge record, include/type.hpp:66-72 (Edge<real_t>, 12 bytes). */
+typedef struct felog_edge12 {
+  uint32_t src;
+  uint32_t dst;
+  float data;
+} felog_edge12;
+#endif
+
+enum { FELOG_FP32 = 0, FELOG_BF16 = 1 };
+enum { FELOG_BUDGET_PLAIN = 0, FELOG_BUDGET_LEARNED = 1 };
+
+typedef struct felog_opts {
+  /* graph and walk flags, include/option_helper.hpp:113-121, :161-165 */
+  uint32_t v_num;           /* -v */
+  uint32_t walker_num;      /* -w; 0 means v_num */
+  uint32_t min_length;      /* --min_L (reference default 20, walk.hpp:416) */
+  uint32_t min_rounds;      /* --min_R (init_round) */
+  uint32_t eval_batch_size; /* --batch_size (accepted, evaluation is one device pass) */
+  int32_t make_undirected;  /* --make-undirected */
+  /* trainer flags, src/word2vec.cu:2269-2286 (defaults word2vec.cu:163-170) */
+  int32_t size;             /* -size (power of two, 32..256) */
+  int32_t window;           /* -window */
+  int32_t negative;         /* -negative (1..15) */
+  int32_t hs;               /* -hs (must be 0) */
+  int32_t cbow;             /* -cbow */
+  int32_t reuse_neg;        /* -reuse-neg */
+  int32_t iter;             /* -iter (parsed, unused like the reference) */
+  int32_t min_count;        /* -min-count */
+  int32_t classes;          /* -classes (K-means output) */
+  int32_t binary;           /* -binary */
+  int32_t debug;            /* -debug */
+  float sample;             /* -sample */
+  float alpha;              /* -alpha (overridden by the LR schedule unless use_cli_alpha) */
+  /* B200 options */
+  int32_t use_cli_alpha;    /* 0: alpha_r = 0.025 e^(-0.1 r) like the reference */
+  int32_t precision;        /* FELOG_FP32 or FELOG_BF16 embedding storage */
+  int32_t deterministic;    /* 1: training runs as one warp in sentence order */
+  int32_t weighted;         /* 1: candidates drawn from the alias table over edge data */
+  int32_t budget_mode;      /* FELOG_BUDGET_PLAIN or FELOG_BUDGET_LEARNED */
+  int32_t max_rounds;       /* felog_run stops after this many rounds (0: no cap) */
+  int32_t device;           /* CUDA device ordinal */
+  int32_t slot_len;         /* tokens reserved per walker before spilling (0: 64) */
+  uint64_t seed;            /* Philox key for walks, neighbour choice, rounding */
+  uint64_t long_arena_tokens; /* spill arena for long walks (0: automatic) */
+  uint64_t wait_limit;      /* spin limit of device-side waits (0: default) */
+} felog_opts;
+
+typedef struct felog_ctx felog_ctx;
+
+/* Injected draws for parity runs: per active walker k (k-th walker in id order
+ * whose start vertex is not stopped), the candidate index draws
+ * idx[idx_off[k] .. idx_off[k+1]) and the trace draws p[p_off[k] .. p_off[k+1])
+ * in the order the walker consumes them (walk.hpp:976, :1005). */
+typedef struct felog_draws {
+  const uint64_t *idx_off;
+  const uint32_t *idx;
+  uint64_t n_idx;
+  const uint64_t *p_off;
+  const double *p;
+  uint64_t n_p;
+  uint64_t n_walkers;
+} felog_draws;
+
+typedef struct felog_walk_stats {
+  uint64_t n_sentences;   /* walkers walked (= corpus sentences) */
+  uint64_t n_tokens;      /* corpus tokens = walk steps incl. step 0 */
+  uint64_t n_traces;      /* go-and-return steps */
+  uint64_t n_iterations;  /* candidate draws */
+  uint64_t n_long;        /* walks that spilled past slot_len */
+  double kl;              /* round relative entropy, walk.hpp:754-787 */
+  float ms;               /* device time of the round's walk kernels */
+} felog_walk_stats;
+
+typedef struct felog_train_stats {
+  uint64_t words;         /* tokens considered by the trainer (before subsampling) */
+  uint64_t kept_words;    /* tokens trained on */
+  uint64_t pairs;         /* (center, context) updates performed */
+  uint64_t sentences;
+  uint64_t batches;
+  float alpha;
+  float ms_plan;
+  float ms_train;
+} felog_train_stats;
+
+typedef struct felog_budget_stats {
+  uint64_t evaluated;     /* vertices checked this round */
+  uint64_t unconverged;   /* evaluated vertices still below the threshold (eva_num) */
+  uint64_t stopped_total; /* vertices whose walkers are stopped */
+  uint64_t predicted;     /* learned mode: vertices decided by the MLP */
+  uint64_t audited;       /* learned mode: vertices re-checked by the plain criterion */
+  uint64_t overruled;     /* learned mode: predictions the plain criterion reversed */
+  int32_t stop_all;       /* 1 when unconverged / previous > 0.7 (word2vec.cu:2073-2078) */
+  float ms;
+} felog_budget_stats;
+
+typedef struct felog_run_stats {
+  uint32_t rounds;
+  uint64_t walk_tokens;
+  uint64_t train_words;
+  double walk_ms;
+  double train_ms;
+  double budget_ms;
+  double total_ms;
+  uint64_t final_unconverged;
+} felog_run_stats;
+
+/* ---- lifecycle ---- */
+void felog_default_opts(felog_opts *opts);
+felog_status felog_create(const felog_opts *opts, felog_ctx **out);
+void felog_destroy(felog_ctx *ctx);
+const char *felog_last_error(const felog_ctx *ctx);
+int felog_abi_version(void);
+
+/* ---- graph ---- */
+/* n records of the 12-byte binary format; doubled (e, e^T interleaved) when
+ * undirected; CSR bucketed by source in record order (graph.hpp:531-575). */
+felog_status felog_load_graph(felog_ctx *ctx, const felog_edge12 *edges, uint64_t n, uint32_t v_num,
+                              int undirected);
+felog_status felog_load_graph_file(felog_ctx *ctx, const char *path, uint32_t v_num, int undirected);
+felog_status felog_graph_info(felog_ctx *ctx, uint32_t *v_num, uint64_t *e_num);
+felog_status felog_get_csr(felog_ctx *ctx, uint64_t *row_ptr, uint32_t *nbr, float *data);
+felog_status felog_get_degrees(felog_ctx *ctx, uint32_t *deg);
+/* Per-vertex alias tables over the edge data (Vose); FELOG_INVALID_ARG for a
+ * negative or non-finite weight. prob/alias: e_num entries, optional. */
+felog_status felog_build_alias(felog_ctx *ctx);
+felog_status felog_get_alias(felog_ctx *ctx, float *prob, uint32_t *alias);
+
+/* ---- walk ---- */
+felog_status felog_set_stop_flags(felog_ctx *ctx, const uint8_t *flags);
+felog_status felog_get_stop_flags(felog_ctx *ctx, uint8_t *flags);
+/* round: 0-based round index (part of the Philox counter). draws: NULL for the
+ * native Philox stream. */
+felog_status felog_walk_round(felog_ctx *ctx, uint32_t round, const felog_draws *draws,
+                              felog_walk_stats *stats);
+felog_status felog_corpus_size(felog_ctx *ctx, uint64_t *n_sentences, uint64_t *n_tokens);
+/* sentences in walker-id order; sent_off: n_sentences + 1 entries */
+felog_status felog_get_corpus(felog_ctx *ctx, uint32_t *tokens, uint64_t tok_cap, uint64_t *sent_off,
+                              uint64_t off_cap);
+/* replace the corpus (training from a given walk file or a test corpus) */
+felog_status felog_set_corpus(felog_ctx *ctx, const uint32_t *tokens, const uint64_t *sent_off,
+                              uint64_t n_sentences);
+felog_status felog_get_visit_freq(felog_ctx *ctx, uint64_t *freq);
+
+/* ---- trainer ---- */
+felog_status felog_init_model(felog_ctx *ctx);
+felog_status felog_vocab_info(felog_ctx *ctx, uint64_t *vocab_size, uint64_t *train_words);
+felog_status felog_get_vocab(felog_ctx *ctx, uint32_t *vocab_vertex, uint32_t *id2offset);
+/* alpha < 0: take the schedule value of round `round` */
+felog_status felog_train_round(felog_ctx *ctx, uint32_t round, float alpha, felog_train_stats *stats);
+/* rows in vocabulary order, logical dimension order, FP32 */
+felog_status felog_get_embeddings(felog_ctx *ctx, float *syn0, float *syn1, uint64_t cap_floats);
+felog_status felog_set_embeddings(felog_ctx *ctx, const float *syn0, const float *syn1);
+/* the batch plan of the last felog_train_round (parity checks) */
+felog_status felog_plan_size(felog_ctx *ctx, uint64_t *n_sentences, uint64_t *n_sen, uint64_t *n_batches);
+felog_status felog_get_plan(felog_ctx *ctx, int32_t *sen, uint64_t *sent_start, uint64_t *batch_first,
+                            int32_t *negs);
+
+/* ---- budget ---- */
+felog_status felog_budget_check(felog_ctx *ctx, uint32_t round, felog_budget_stats *stats);
+felog_status felog_get_similarity(felog_ctx *ctx, float *sim);
+
+/* ---- whole loop ---- */
+felog_status felog_run(felog_ctx *ctx, felog_run_stats *stats);
+felog_status felog_write_embeddings(felog_ctx *ctx, const char *path);
+
+/* Kernels this library has launched on the context (diagnostics). */
+uint64_t felog_kernel_launches(const felog_ctx *ctx);
+/* Device timer on the context's stream: mark(0) records the start event,
+ * mark(1) the stop event; elapsed() synchronizes and returns milliseconds. */
+felog_status felog_timer_mark(felog_ctx *ctx, int which);
+felog_status felog_timer_elapsed(felog_ctx *ctx, float *ms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

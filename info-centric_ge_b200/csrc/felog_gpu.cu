@@ -1,0 +1,1168 @@
+// C ABI of the B200 FeLoG hot path (declarations and reference seams in
+// include/felog_gpu.h).  One felog_ctx owns one device's resident state and a
+// stream; kernels live in the .cuh files next to this one.
+#include "felog_gpu.h"
+
+#include <cub/cub.cuh>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "budget.cuh"
+#include "common.cuh"
+#include "graph.cuh"
+#include "plan.cuh"
+#include "sgns.cuh"
+#include "walk.cuh"
+
+using namespace felog;
+
+namespace {
+
+constexpr int64_t kTableSize = 100000000;  // table_size, word2vec.cu:171
+
+template <class T>
+struct DevBuf {
+  T *p = nullptr;
+  size_t n = 0;
+  cudaError_t ensure(size_t want) {
+    if (want <= n && p) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+    size_t bytes = std::max<size_t>(want, 1) * sizeof(T);
+    cudaError_t e = cudaMalloc(&p, bytes);
+    if (e == cudaSuccess) n = std::max<size_t>(want, 1);
+    return e;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+};
+
+struct Status {
+  felog_status s = FELOG_OK;
+};
+
+}  // namespace
+
+struct felog_ctx {
+  felog_opts o;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaEvent_t tm0 = nullptr, tm1 = nullptr;  // user timer (felog_timer_mark)
+  std::string err;
+  int sm_count = 148;
+
+  // graph
+  uint32_t V = 0;
+  uint64_t M = 0;
+  DevBuf<uint64_t> row_ptr;
+  DevBuf<uint2> adj;
+  DevBuf<uint32_t> deg;
+  std::vector<uint32_t> h_deg;
+  DevBuf<float> alias_prob;
+  DevBuf<uint32_t> alias_idx;
+  bool has_alias = false;
+
+  // walk
+  DevBuf<uint8_t> stop;
+  DevBuf<uint32_t> active;
+  uint32_t n_active = 0;
+  DevBuf<uint32_t> arena;
+  uint64_t arena_cap = 0;
+  uint64_t spill_base = 0;
+  DevBuf<uint64_t> sent_ptr;
+  DevBuf<uint32_t> sent_len;
+  uint64_t n_sent = 0, n_tok = 0;
+  bool corpus_ready = false;
+  DevBuf<unsigned int> visit_freq;
+  uint64_t words_sum_cum = 0;
+  DevBuf<unsigned long long> counters;  // scratch counters
+  DevBuf<int> derr;
+  DevBuf<uint64_t> inj_idx_off, inj_p_off;
+  DevBuf<uint32_t> inj_idx;
+  DevBuf<double> inj_p;
+  DevBuf<uint32_t> flags_tmp;
+  DevBuf<double> kl_partial;
+
+  // vocabulary / model
+  long long vocab_size = 0, train_words = 0;
+  std::vector<uint32_t> h_vocab_vertex, h_id2offset;
+  DevBuf<uint32_t> id2offset;
+  DevBuf<uint16_t> thr;
+  bool use_thr = false;
+  DevBuf<int32_t> table;
+  DevBuf<float> exp_table;
+  DevBuf<float> syn0, syn1;
+  bool model_ready = false;
+  DevBuf<LcgJump> jump;
+
+  // plan
+  DevBuf<uint32_t> p_cand, p_draws, p_cons, p_kept, p_blk;
+  DevBuf<unsigned long long> p_state, p_neg_state;
+  DevBuf<uint64_t> p_out_off, p_batch_first;
+  DevBuf<int32_t> p_sen, p_negs;
+  uint64_t plan_sent = 0, plan_sen = 0, plan_batches = 0;
+
+  // budget
+  DevBuf<float> sim;
+  uint64_t last_eva = 0;
+  bool have_last_eva = false;
+
+  // cub scratch, output staging, launch count of this library's kernels
+  DevBuf<unsigned char> cub_tmp;
+  DevBuf<float> out_tmp;
+  uint64_t launches = 0;
+};
+
+namespace {
+
+felog_status fail(felog_ctx *c, felog_status s, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  if (c) c->err = buf;
+  return s;
+}
+
+felog_status cuda_fail(felog_ctx *c, cudaError_t e, const char *what) {
+  if (e == cudaErrorMemoryAllocation) {
+    cudaGetLastError();
+    return fail(c, FELOG_OOM, "%s: out of device memory", what);
+  }
+  return fail(c, FELOG_CUDA_ERROR, "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define CK(expr, what)                                   \
+  do {                                                   \
+    cudaError_t _e = (expr);                             \
+    if (_e != cudaSuccess) return cuda_fail(c, _e, what); \
+  } while (0)
+
+int grid_for(felog_ctx *c, uint64_t n, int threads, int per_sm = 8) {
+  uint64_t g = (n + threads - 1) / threads;
+  uint64_t cap = (uint64_t)c->sm_count * per_sm;
+  if (g > cap) g = cap;
+  if (g < 1) g = 1;
+  return (int)g;
+}
+
+felog_status check_dev_err(felog_ctx *c, const char *what) {
+  int h = 0;
+  CK(cudaMemcpyAsync(&h, c->derr.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream), what);
+  CK(cudaStreamSynchronize(c->stream), what);
+  if (h == kErrNone) return FELOG_OK;
+  CK(cudaMemsetAsync(c->derr.p, 0, sizeof(int), c->stream), what);
+  switch (h) {
+    case kErrDrawsExhausted: return fail(c, FELOG_INVALID_ARG, "%s: injected draws exhausted or out of range", what);
+    case kErrArenaFull: return fail(c, FELOG_OOM, "%s: spill arena for long walks exhausted", what);
+    case kErrBadVertex: return fail(c, FELOG_INVALID_ARG, "%s: edge endpoint >= v_num", what);
+    case kErrWaitTimeout: return fail(c, FELOG_DEVICE_TIMEOUT, "%s: device wait timed out", what);
+    case kErrBadWeight: return fail(c, FELOG_INVALID_ARG, "%s: negative or non-finite edge weight", what);
+    case kErrPlanOverflow: return fail(c, FELOG_INTERNAL, "%s: batch plan overflow", what);
+    case kErrWalkLimit:
+      return fail(c, FELOG_INVALID_ARG, "%s: a walker exceeded %u draws (start vertex whose only neighbour is itself)",
+                  what, kWalkIterLimit);
+    default: return fail(c, FELOG_INTERNAL, "%s: device error %d", what, h);
+  }
+}
+
+bool dim_ok(int d) { return d == 32 || d == 64 || d == 128 || d == 256; }
+
+// logical <-> interleaved row layout (see sgns.cuh)
+inline size_t phys_index(int dim, int logical) {
+  int J = dim / 32;
+  int lane = logical % 32, j = logical / 32;
+  return (size_t)lane * J + j;
+}
+
+}  // namespace
+
+// =================================================================== ABI
+
+extern "C" int felog_abi_version(void) { return FELOG_ABI_VERSION; }
+
+extern "C" void felog_default_opts(felog_opts *o) {
+  memset(o, 0, sizeof(*o));
+  o->min_length = 20;  // walk.hpp:416
+  o->min_rounds = 5;   // walk.hpp:417
+  o->eval_batch_size = 16384;
+  o->make_undirected = 0;
+  o->size = 100;       // word2vec.cu:164
+  o->window = 5;
+  o->negative = 5;
+  o->hs = 0;
+  o->cbow = 1;         // word2vec.cu:163
+  o->reuse_neg = 1;
+  o->iter = 5;
+  o->min_count = 5;
+  o->classes = 0;
+  o->binary = 0;
+  o->debug = 2;
+  o->sample = 1e-3f;
+  o->alpha = 0.025f;
+  o->precision = FELOG_FP32;
+  o->seed = 0x5EED0001ULL;
+  o->slot_len = 64;
+}
+
+extern "C" felog_status felog_create(const felog_opts *opts, felog_ctx **out) {
+  if (!opts || !out) return FELOG_INVALID_ARG;
+  *out = nullptr;
+  felog_ctx *c = new (std::nothrow) felog_ctx();
+  if (!c) return FELOG_OOM;
+  c->o = *opts;
+  if (c->o.slot_len <= 0) c->o.slot_len = 64;
+  c->o.slot_len = (c->o.slot_len + 3) & ~3;
+  c->device = opts->device;
+  cudaError_t e = cudaSetDevice(c->device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreate(&c->ev0);
+  if (e == cudaSuccess) e = cudaEventCreate(&c->ev1);
+  if (e == cudaSuccess) e = cudaEventCreate(&c->tm0);
+  if (e == cudaSuccess) e = cudaEventCreate(&c->tm1);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, c->device);
+  if (e == cudaSuccess) e = c->counters.ensure(16);
+  if (e == cudaSuccess) e = c->derr.ensure(1);
+  if (e == cudaSuccess) e = cudaMemset(c->derr.p, 0, sizeof(int));
+  if (e == cudaSuccess) {
+    LcgJump j;
+    lcg_jump_table(j);
+    e = c->jump.ensure(1);
+    if (e == cudaSuccess) e = cudaMemcpy(c->jump.p, &j, sizeof j, cudaMemcpyHostToDevice);
+  }
+  if (e != cudaSuccess) {
+    felog_status s = e == cudaErrorMemoryAllocation ? FELOG_OOM : FELOG_CUDA_ERROR;
+    felog_destroy(c);
+    return s;
+  }
+  *out = c;
+  return FELOG_OK;
+}
+
+extern "C" void felog_destroy(felog_ctx *c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  c->row_ptr.release(); c->adj.release(); c->deg.release(); c->alias_prob.release(); c->alias_idx.release();
+  c->stop.release(); c->active.release(); c->arena.release(); c->sent_ptr.release(); c->sent_len.release();
+  c->visit_freq.release(); c->counters.release(); c->derr.release(); c->inj_idx_off.release();
+  c->inj_p_off.release(); c->inj_idx.release(); c->inj_p.release(); c->flags_tmp.release();
+  c->kl_partial.release(); c->id2offset.release(); c->thr.release(); c->table.release();
+  c->exp_table.release(); c->syn0.release(); c->syn1.release(); c->jump.release();
+  c->p_cand.release(); c->p_draws.release(); c->p_cons.release(); c->p_kept.release(); c->p_blk.release();
+  c->p_state.release(); c->p_neg_state.release(); c->p_out_off.release(); c->p_batch_first.release();
+  c->p_sen.release(); c->p_negs.release(); c->sim.release(); c->cub_tmp.release(); c->out_tmp.release();
+  if (c->ev0) cudaEventDestroy(c->ev0);
+  if (c->ev1) cudaEventDestroy(c->ev1);
+  if (c->tm0) cudaEventDestroy(c->tm0);
+  if (c->tm1) cudaEventDestroy(c->tm1);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+}
+
+extern "C" const char *felog_last_error(const felog_ctx *c) { return c ? c->err.c_str() : "null context"; }
+
+// ----------------------------------------------------------------- graph
+
+extern "C" felog_status felog_load_graph(felog_ctx *c, const felog_edge12 *edges, uint64_t n, uint32_t v_num,
+                                         int undirected) {
+  if (!c) return FELOG_INVALID_ARG;
+  if (v_num == 0) return fail(c, FELOG_INVALID_ARG, "load_graph: v_num must be > 0");
+  if (n && !edges) return fail(c, FELOG_INVALID_ARG, "load_graph: edges is NULL");
+  uint64_t m = undirected ? 2 * n : n;
+  if (m >= 0xFFFFFFFFULL) return fail(c, FELOG_INVALID_ARG, "load_graph: more than 2^32-1 CSR entries");
+  // the previous graph is gone as soon as its buffers are reused
+  c->V = 0;
+  c->M = 0;
+  c->model_ready = false;
+  c->corpus_ready = false;
+  c->has_alias = false;
+  CK(cudaSetDevice(c->device), "load_graph");
+  DevBuf<uint32_t> rec, keys, vals, keys2, vals2;
+  CK(rec.ensure(3 * std::max<uint64_t>(n, 1)), "load_graph: records");
+  if (n) CK(cudaMemcpyAsync(rec.p, edges, n * 12, cudaMemcpyHostToDevice, c->stream), "load_graph: upload");
+  CK(keys.ensure(m), "load_graph");
+  CK(vals.ensure(m), "load_graph");
+  CK(keys2.ensure(m), "load_graph");
+  CK(vals2.ensure(m), "load_graph");
+  CK(c->deg.ensure(v_num), "load_graph");
+  CK(c->row_ptr.ensure((size_t)v_num + 1), "load_graph");
+  CK(c->adj.ensure(m), "load_graph");
+  CK(cudaMemsetAsync(c->deg.p, 0, sizeof(uint32_t) * v_num, c->stream), "load_graph");
+  CK(cudaMemsetAsync(c->derr.p, 0, sizeof(int), c->stream), "load_graph");
+  if (m) {
+    k_expand_edges<<<grid_for(c, m, 256), 256, 0, c->stream>>>(rec.p, n, undirected, v_num, keys.p, vals.p,
+                                                                  c->deg.p, c->derr.p);
+    c->launches++;
+    CK(cudaGetLastError(), "load_graph: expand");
+    int end_bit = 1;
+    while (end_bit < 32 && (1ULL << end_bit) < v_num) end_bit++;
+    cub::DoubleBuffer<uint32_t> dk(keys.p, keys2.p), dv(vals.p, vals2.p);
+    size_t tmp = 0;
+    CK(cub::DeviceRadixSort::SortPairs(nullptr, tmp, dk, dv, (int)m, 0, end_bit, c->stream), "load_graph: sort");
+    CK(c->cub_tmp.ensure(tmp), "load_graph: sort scratch");
+    CK(cub::DeviceRadixSort::SortPairs(c->cub_tmp.p, tmp, dk, dv, (int)m, 0, end_bit, c->stream),
+       "load_graph: sort");
+    k_gather_adj<<<grid_for(c, m, 256), 256, 0, c->stream>>>(rec.p, dv.Current(), m, undirected, c->adj.p);
+    c->launches++;
+    CK(cudaGetLastError(), "load_graph: gather");
+  }
+  // row_ptr = exclusive scan of degrees (u32 -> u64)
+  {
+    CK(cudaMemsetAsync(c->row_ptr.p, 0, sizeof(uint64_t), c->stream), "load_graph");
+    size_t tmp = 0;
+    CK(cub::DeviceScan::InclusiveSum(nullptr, tmp, c->deg.p, c->row_ptr.p + 1, (int)v_num, c->stream),
+       "load_graph: scan");
+    CK(c->cub_tmp.ensure(tmp), "load_graph: scan scratch");
+    CK(cub::DeviceScan::InclusiveSum(c->cub_tmp.p, tmp, c->deg.p, c->row_ptr.p + 1, (int)v_num, c->stream),
+       "load_graph: scan");
+  }
+  felog_status s = check_dev_err(c, "load_graph");
+  if (s != FELOG_OK) return s;
+  c->h_deg.resize(v_num);
+  CK(cudaMemcpyAsync(c->h_deg.data(), c->deg.p, sizeof(uint32_t) * v_num, cudaMemcpyDeviceToHost, c->stream),
+     "load_graph");
+  CK(cudaStreamSynchronize(c->stream), "load_graph");
+  rec.release(); keys.release(); vals.release(); keys2.release(); vals2.release();
+  c->V = v_num;
+  c->M = m;
+  c->has_alias = false;
+  c->model_ready = false;
+  c->corpus_ready = false;
+  c->have_last_eva = false;
+  c->words_sum_cum = 0;
+  CK(c->stop.ensure(v_num), "load_graph");
+  CK(cudaMemsetAsync(c->stop.p, 0, v_num, c->stream), "load_graph");
+  CK(c->visit_freq.ensure(v_num), "load_graph");
+  CK(cudaMemsetAsync(c->visit_freq.p, 0, sizeof(unsigned int) * v_num, c->stream), "load_graph");
+  CK(cudaStreamSynchronize(c->stream), "load_graph");
+  return FELOG_OK;
+}
+
+extern "C" felog_status felog_load_graph_file(felog_ctx *c, const char *path, uint32_t v_num, int undirected) {
+  if (!c || !path) return FELOG_INVALID_ARG;
+  FILE *f = fopen(path, "rb");
+  if (!f) return fail(c, FELOG_IO_ERROR, "cannot open graph file %s", path);
+  fseek(f, 0, SEEK_END);
+  long sz = ftell(f);
+  fseek(f, 0, SEEK_SET);
+  if (sz < 0) {
+    fclose(f);
+    return fail(c, FELOG_IO_ERROR, "cannot size graph file %s", path);
+  }
+  size_t n = (size_t)sz / sizeof(felog_edge12);  // whole records only, storage.hpp:49-52
+  std::vector<felog_edge12> e(n);
+  size_t got = n ? fread(e.data(), sizeof(felog_edge12), n, f) : 0;
+  fclose(f);
+  if (got != n) return fail(c, FELOG_IO_ERROR, "short read on %s", path);
+  return felog_load_graph(c, e.data(), n, v_num, undirected);
+}
+
+extern "C" felog_status felog_graph_info(felog_ctx *c, uint32_t *v_num, uint64_t *e_num) {
+  if (!c) return FELOG_INVALID_ARG;
+  if (v_num) *v_num = c->V;
+  if (e_num) *e_num = c->M;
+  return FELOG_OK;
+}
+
+extern "C" felog_status felog_get_csr(felog_ctx *c, uint64_t *row_ptr, uint32_t *nbr, float *data) {
+  if (!c || !c->V) return c ? fail(c, FELOG_NOT_READY, "no graph loaded") : FELOG_INVALID_ARG;
+  if (row_ptr)
+    CK(cudaMemcpy(row_ptr, c->row_ptr.p, sizeof(uint64_t) * (c->V + 1ULL), cudaMemcpyDeviceToHost), "get_csr");
+  if ((nbr || data) && c->M) {
+    std::vector<uint2> a(c->M);
+    CK(cudaMemcpy(a.data(), c->adj.p, sizeof(uint2) * c->M, cudaMemcpyDeviceToHost), "get_csr");
+    for (uint64_t i = 0; i < c->M; i++) {
+      if (nbr) nbr[i] = a[i].x;
+      if (data) memcpy(&data[i], &a[i].y, 4);
+    }
+  }
+  return FELOG_OK;
+}
+
+extern "C" felog_status felog_get_degrees(felog_ctx *c, uint32_t *deg) {
+  if (!c || !deg) return FELOG_INVALID_ARG;
+  if (!c->V) return fail(c, FELOG_NOT_READY, "no graph loaded");
+  memcpy(deg, c->h_deg.data(), sizeof(uint32_t) * c->V);
+  return FELOG_OK;
+}
+
+extern "C" felog_status felog_build_alias(felog_ctx *c) {
+  if (!c) return FELOG_INVALID_ARG;
+  if (!c->V) return fail(c, FELOG_NOT_READY, "no graph loaded");
+  CK(cudaSetDevice(c->device), "build_alias");
+  CK(c->alias_prob.ensure(c->M), "build_alias");
+  CK(c->alias_idx.ensure(c->M), "build_alias");
+  DevBuf<uint32_t> scratch;
+  CK(scratch.ensure(c->M), "build_alias");
+  CK(cudaMemsetAsync(c->derr.p, 0, sizeof(int), c->stream), "build_alias");
+  k_build_alias<<<grid_for(c, (uint64_t)c->V * 32, 256), 256, 0, c->stream>>>(c->row_ptr.p, c->adj.p, c->V,
+                                                                              c->alias_prob.p, c->alias_idx.p,
+                                                                              scratch.p, c->derr.p);
+  c->launches++;
+  CK(cudaGetLastError(), "build_alias");
+  felog_status s = check_dev_err(c, "build_alias");
+  scratch.release();
+  if (s != FELOG_OK) return s;
+  c->has_alias = true;
+  return FELOG_OK;
+}
+
+extern "C" felog_status felog_get_alias(felog_ctx *c, float *prob, uint32_t *alias) {
+  if (!c) return FELOG_INVALID_ARG;
+  if (!c->has_alias) return fail(c, FELOG_NOT_READY, "alias tables not built");
+  if (prob) CK(cudaMemcpy(prob, c->alias_prob.p, 4 * c->M, cudaMemcpyDeviceToHost), "get_alias");
+  if (alias) CK(cudaMemcpy(alias, c->alias_idx.p, 4 * c->M, cudaMemcpyDeviceToHost), "get_alias");
+  return FELOG_OK;
+}
+
+// ------------------------------------------------------------------ walk
+
+extern "C" felog_status felog_set_stop_flags(felog_ctx *c, const uint8_t *flags) {
+  if (!c || !flags) return FELOG_INVALID_ARG;
+  if (!c->V) return fail(c, FELOG_NOT_READY, "no graph loaded");
+  CK(cudaMemcpy(c->stop.p, flags, c->V, cudaMemcpyHostToDevice), "set_stop_flags");
+  return FELOG_OK;
+}
+
+extern "C" felog_status felog_get_stop_flags(felog_ctx *c, uint8_t *flags) {
+  if (!c || !flags) return FELOG_INVALID_ARG;
+  if (!c->V) return fail(c, FELOG_NOT_READY, "no graph loaded");
+  CK(cudaMemcpy(flags, c->stop.p, c->V, cudaMemcpyDeviceToHost), "get_stop_flags");
+  return FELOG_OK;
+}
+
+namespace {
+
+__global__ void k_active_flags(const uint8_t *stop, uint32_t v_num, uint32_t walker_num, uint32_t *flag) {
+  for (uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w < walker_num; w += gridDim.x * blockDim.x)
+    flag[w] = stop[w % v_num] ? 0u : 1u;
+}
+
+__global__ void k_active_scatter(const uint32_t *flag, const uint32_t *pos, uint32_t walker_num, uint32_t *active) {
+  for (uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w < walker_num; w += gridDim.x * blockDim.x)
+    if (flag[w]) active[pos[w]] = w;
+}
+
+// walkers whose start vertex is not stopped, ascending (walk.hpp:563-572)
+felog_status build_active(felog_ctx *c, uint32_t walker_num) {
+  CK(c->flags_tmp.ensure(2 * (size_t)walker_num + 2), "walk_round: active");
+  CK(c->active.ensure(walker_num), "walk_round: active");
+  uint32_t *flag = c->flags_tmp.p, *pos = c->flags_tmp.p + walker_num + 1;
+  k_active_flags<<<grid_for(c, walker_num, 256), 256, 0, c->stream>>>(c->stop.p, c->V, walker_num, flag);
+  c->launches++;
+  size_t tmp = 0;
+  CK(cub::DeviceScan::ExclusiveSum(nullptr, tmp, flag, pos, (int)walker_num + 1, c->stream), "walk_round: scan");
+  CK(c->cub_tmp.ensure(tmp), "walk_round: scan");
+  CK(cudaMemsetAsync(flag + walker_num, 0, sizeof(uint32_t), c->stream), "walk_round");
+  CK(cub::DeviceScan::ExclusiveSum(c->cub_tmp.p, tmp, flag, pos, (int)walker_num + 1, c->stream),
+     "walk_round: scan");
+  k_active_scatter<<<grid_for(c, walker_num, 256), 256, 0, c->stream>>>(flag, pos, walker_num, c->active.p);
+  c->launches++;
+  uint32_t na = 0;
+  CK(cudaMemcpyAsync(&na, pos + walker_num, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream), "walk_round");
+  CK(cudaStreamSynchronize(c->stream), "walk_round");
+  c->n_active = na;
+  return FELOG_OK;
+}
+
+felog_status round_kl(felog_ctx *c, double *out) {
+  const int nb = 256;
+  CK(c->kl_partial.ensure(nb + 1), "kl");
+  double deg_sum = (double)c->M;
+  double words = (double)c->words_sum_cum;
+  if (words <= 0) {
+    *out = NAN;
+    return FELOG_OK;
+  }
+  k_kl_partial<<<nb, 256, 0, c->stream>>>(c->deg.p, c->visit_freq.p, c->V, deg_sum, words, c->kl_partial.p);
+  c->launches++;
+  k_kl_final<<<1, 32, 0, c->stream>>>(c->kl_partial.p, nb, c->kl_partial.p + nb);
+  c->launches++;
+  CK(cudaMemcpyAsync(out, c->kl_partial.p + nb, sizeof(double), cudaMemcpyDeviceToHost, c->stream), "kl");
+  CK(cudaStreamSynchronize(c->stream), "kl");
+  return FELOG_OK;
+}
+
+}  // namespace
+
+extern "C" felog_status felog_walk_round(felog_ctx *c, uint32_t round, const felog_draws *draws,
+                                         felog_walk_stats *stats) {
+  if (!c) return FELOG_INVALID_ARG;
+  if (!c->V) return fail(c, FELOG_NOT_READY, "no graph loaded");
+  if (c->o.weighted && !c->has_alias) return fail(c, FELOG_NOT_READY, "weighted walk needs felog_build_alias");
+  CK(cudaSetDevice(c->device), "walk_round");
+  const uint32_t walker_num = c->o.walker_num ? c->o.walker_num : c->V;
+  felog_status s = build_active(c, walker_num);
+  if (s != FELOG_OK) return s;
+  const uint32_t na = c->n_active;
+  if (draws && draws->n_walkers != na)
+    return fail(c, FELOG_INVALID_ARG, "walk_round: draws cover %llu walkers, %u are active",
+                (unsigned long long)draws->n_walkers, na);
+  const uint64_t slot = (uint64_t)c->o.slot_len;
+  uint64_t spill = c->o.long_arena_tokens ? c->o.long_arena_tokens
+                                          : std::max<uint64_t>(1u << 20, (uint64_t)na * slot / 8);
+  spill = (spill + 3) & ~3ULL;
+  c->spill_base = (uint64_t)na * slot;
+  c->arena_cap = c->spill_base + spill;
+  CK(c->arena.ensure(c->arena_cap), "walk_round: arena");
+  CK(c->sent_ptr.ensure((size_t)na + 1), "walk_round");
+  CK(c->sent_len.ensure((size_t)na + 1), "walk_round");
+  if (draws) {
+    CK(c->inj_idx_off.ensure((size_t)na + 1), "walk_round: draws");
+    CK(c->inj_p_off.ensure((size_t)na + 1), "walk_round: draws");
+    CK(c->inj_idx.ensure(draws->n_idx), "walk_round: draws");
+    CK(c->inj_p.ensure(draws->n_p), "walk_round: draws");
+    CK(cudaMemcpyAsync(c->inj_idx_off.p, draws->idx_off, 8 * ((size_t)na + 1), cudaMemcpyHostToDevice, c->stream),
+       "walk_round: draws");
+    CK(cudaMemcpyAsync(c->inj_p_off.p, draws->p_off, 8 * ((size_t)na + 1), cudaMemcpyHostToDevice, c->stream),
+       "walk_round: draws");
+    if (draws->n_idx)
+      CK(cudaMemcpyAsync(c->inj_idx.p, draws->idx, 4 * draws->n_idx, cudaMemcpyHostToDevice, c->stream),
+         "walk_round: draws");
+    if (draws->n_p)
+      CK(cudaMemcpyAsync(c->inj_p.p, draws->p, 8 * draws->n_p, cudaMemcpyHostToDevice, c->stream),
+         "walk_round: draws");
+  }
+  CK(cudaMemsetAsync(c->counters.p, 0, sizeof(unsigned long long) * 16, c->stream), "walk_round");
+  CK(cudaMemsetAsync(c->derr.p, 0, sizeof(int), c->stream), "walk_round");
+  WalkArgs a{};
+  a.row_ptr = c->row_ptr.p;
+  a.adj = c->adj.p;
+  a.alias_prob = c->alias_prob.p;
+  a.alias_idx = c->alias_idx.p;
+  a.v_num = c->V;
+  a.n_active = na;
+  a.active = c->active.p;
+  a.min_len = c->o.min_length;
+  a.round = round;
+  a.seed = c->o.seed;
+  a.weighted = c->o.weighted && !draws;
+  a.injected = draws != nullptr;
+  a.inj_idx_off = c->inj_idx_off.p;
+  a.inj_idx = c->inj_idx.p;
+  a.inj_p_off = c->inj_p_off.p;
+  a.inj_p = c->inj_p.p;
+  a.arena = c->arena.p;
+  a.slot_len = (uint32_t)slot;
+  a.spill_cursor = c->counters.p + 8;
+  a.spill_base = c->spill_base;
+  a.arena_cap = c->arena_cap;
+  a.sent_ptr = c->sent_ptr.p;
+  a.sent_len = c->sent_len.p;
+  a.visit_freq = c->visit_freq.p;
+  a.next_walker = reinterpret_cast<unsigned int *>(c->counters.p + 9);
+  a.stats = c->counters.p;
+  a.err = c->derr.p;
+  CK(cudaEventRecord(c->ev0, c->stream), "walk_round");
+  if (na) {
+    int blocks = c->sm_count * 8;
+    k_walk<<<blocks, 256, 0, c->stream>>>(a);
+    c->launches++;
+    CK(cudaGetLastError(), "walk_round: launch");
+  }
+  CK(cudaEventRecord(c->ev1, c->stream), "walk_round");
+  unsigned long long h[16];
+  CK(cudaMemcpyAsync(h, c->counters.p, sizeof h, cudaMemcpyDeviceToHost, c->stream), "walk_round");
+  s = check_dev_err(c, "walk_round");
+  if (s != FELOG_OK) return s;
+  float ms = 0;
+  CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1), "walk_round");
+  c->n_sent = na;
+  c->n_tok = h[0];
+  c->corpus_ready = true;
+  c->words_sum_cum += h[0];
+  if (stats) {
+    memset(stats, 0, sizeof(*stats));
+    stats->n_sentences = na;
+    stats->n_tokens = h[0];
+    stats->n_traces = h[1];
+    stats->n_iterations = h[2];
+    stats->n_long = h[3];
+    stats->ms = ms;
+    s = round_kl(c, &stats->kl);
+    if (s != FELOG_OK) return s;
+  }
+  return FELOG_OK;
+}
+
+extern "C" felog_status felog_corpus_size(felog_ctx *c, uint64_t *n_sentences, uint64_t *n_tokens) {
+  if (!c) return FELOG_INVALID_ARG;
+  if (!c->corpus_ready) return fail(c, FELOG_NOT_READY, "no corpus");
+  if (n_sentences) *n_sentences = c->n_sent;
+  if (n_tokens) *n_tokens = c->n_tok;
+  return FELOG_OK;
+}
+
+extern "C" felog_status felog_get_corpus(felog_ctx *c, uint32_t *tokens, uint64_t tok_cap, uint64_t *sent_off,
+                                         uint64_t off_cap) {
+  if (!c) return FELOG_INVALID_ARG;
+  if (!c->corpus_ready) return fail(c, FELOG_NOT_READY, "no corpus");
+  if (tok_cap < c->n_tok || off_cap < c->n_sent + 1)
+    return fail(c, FELOG_INVALID_ARG, "get_corpus: buffers too small (%llu tokens, %llu sentences)",
+                (unsigned long long)c->n_tok, (unsigned long long)c->n_sent);
+  std::vector<uint64_t> ptr(c->n_sent);
+  std::vector<uint32_t> len(c->n_sent);
+  if (c->n_sent) {
+    CK(cudaMemcpy(ptr.data(), c->sent_ptr.p, 8 * c->n_sent, cudaMemcpyDeviceToHost), "get_corpus");
+    CK(cudaMemcpy(len.data(), c->sent_len.p, 4 * c->n_sent, cudaMemcpyDeviceToHost), "get_corpus");
+  }
+  std::vector<uint32_t> ar(c->arena_cap);
+  if (c->arena_cap) CK(cudaMemcpy(ar.data(), c->arena.p, 4 * c->arena_cap, cudaMemcpyDeviceToHost), "get_corpus");
+  uint64_t o = 0;
+  sent_off[0] = 0;
+  for (uint64_t k = 0; k < c->n_sent; k++) {
+    memcpy(tokens + o, ar.data() + ptr[k], 4 * (size_t)len[k]);
+    o += len[k];
+    sent_off[k + 1] = o;
+  }
+  return FELOG_OK;
+}
+
+extern "C" felog_status felog_set_corpus(felog_ctx *c, const uint32_t *tokens, const uint64_t *sent_off,
+                                         uint64_t n_sentences) {
+  if (!c || !sent_off || (n_sentences && !tokens)) return FELOG_INVALID_ARG;
+  if (!c->V) return fail(c, FELOG_NOT_READY, "no graph loaded");
+  uint64_t ntok = sent_off[n_sentences];
+  for (uint64_t k = 0; k < n_sentences; k++)
+    if (sent_off[k + 1] < sent_off[k]) return fail(c, FELOG_INVALID_ARG, "set_corpus: offsets not ascending");
+  for (uint64_t t = 0; t < ntok; t++)
+    if (tokens[t] >= c->V) return fail(c, FELOG_INVALID_ARG, "set_corpus: token %llu out of range",
+                                       (unsigned long long)t);
+  CK(c->arena.ensure(std::max<uint64_t>(ntok, 4)), "set_corpus");
+  CK(c->sent_ptr.ensure(n_sentences + 1), "set_corpus");
+  CK(c->sent_len.ensure(n_sentences + 1), "set_corpus");
+  std::vector<uint64_t> ptr(n_sentences);
+  std::vector<uint32_t> len(n_sentences);
+  for (uint64_t k = 0; k < n_sentences; k++) {
+    ptr[k] = sent_off[k];
+    len[k] = (uint32_t)(sent_off[k + 1] - sent_off[k]);
+  }
+  if (ntok) CK(cudaMemcpy(c->arena.p, tokens, 4 * ntok, cudaMemcpyHostToDevice), "set_corpus");
+  if (n_sentences) {
+    CK(cudaMemcpy(c->sent_ptr.p, ptr.data(), 8 * n_sentences, cudaMemcpyHostToDevice), "set_corpus");
+    CK(cudaMemcpy(c->sent_len.p, len.data(), 4 * n_sentences, cudaMemcpyHostToDevice), "set_corpus");
+  }
+  c->arena_cap = std::max<uint64_t>(ntok, 4);
+  c->n_sent = n_sentences;
+  c->n_tok = ntok;
+  c->corpus_ready = true;
+  return FELOG_OK;
+}
+
+extern "C" felog_status felog_get_visit_freq(felog_ctx *c, uint64_t *freq) {
+  if (!c || !freq) return FELOG_INVALID_ARG;
+  if (!c->V) return fail(c, FELOG_NOT_READY, "no graph loaded");
+  std::vector<unsigned int> f(c->V);
+  CK(cudaMemcpy(f.data(), c->visit_freq.p, 4 * (size_t)c->V, cudaMemcpyDeviceToHost), "get_visit_freq");
+  for (uint32_t v = 0; v < c->V; v++) freq[v] = f[v];
+  return FELOG_OK;
+}
+
+// --------------------------------------------------------------- trainer
+
+namespace {
+
+__global__ void k_init_syn0(float *syn0, uint64_t vocab_size, int dim, const LcgJump *J) {
+  const uint64_t n = vocab_size * (uint64_t)dim;
+  const int Jn = dim / 32;
+  for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < n; e += (uint64_t)gridDim.x * blockDim.x) {
+    // element e of the row-major LCG fill (word2vec.cu:893-896): state after e + 1 steps from 1
+    unsigned long long s = lcg_jump(*J, 1ULL, e + 1);
+    float q = __fdiv_rn((float)(s & 0xFFFF), 65536.0f);
+    float v = (float)__ddiv_rn(__dsub_rn((double)q, 0.5), (double)dim);
+    uint64_t row = e / dim;
+    int logical = (int)(e % dim);
+    syn0[row * dim + (uint64_t)(logical % 32) * Jn + logical / 32] = v;
+  }
+}
+
+}  // namespace
+
+extern "C" felog_status felog_init_model(felog_ctx *c) {
+  if (!c) return FELOG_INVALID_ARG;
+  if (!c->V) return fail(c, FELOG_NOT_READY, "no graph loaded");
+  const int dim = c->o.size;
+  if (!dim_ok(dim)) return fail(c, FELOG_INVALID_ARG, "-size %d: supported sizes are 32, 64, 128, 256", dim);
+  if (c->o.hs) return fail(c, FELOG_INVALID_ARG, "-hs 1 is not supported; use negative sampling");
+  if (c->o.negative < 1 || c->o.negative > kMaxNeg)
+    return fail(c, FELOG_INVALID_ARG, "-negative %d: supported range is 1..%d", c->o.negative, kMaxNeg);
+  if (c->o.window < 1) return fail(c, FELOG_INVALID_ARG, "-window must be >= 1");
+  if (c->o.precision != FELOG_FP32) return fail(c, FELOG_INVALID_ARG, "precision mode not available");
+  CK(cudaSetDevice(c->device), "init_model");
+  // vocabulary from degrees: stable sort, degree descending (word2vec.cu:834-862, :734-755)
+  const uint32_t V = c->V;
+  std::vector<uint32_t> order(V);
+  std::iota(order.begin(), order.end(), 0u);
+  std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return c->h_deg[a] > c->h_deg[b]; });
+  long long size = V, tw = 0;
+  for (uint32_t i = 0; i < V; i++) {
+    if ((long long)c->h_deg[order[i]] < c->o.min_count && i != 0) size--;
+    else tw += c->h_deg[order[i]];
+  }
+  if (size < 2) return fail(c, FELOG_INVALID_ARG, "vocabulary has fewer than 2 words");
+  c->h_vocab_vertex.assign(order.begin(), order.begin() + size);
+  c->h_id2offset.assign(V, 0xFFFFFFFFu);
+  for (long long i = 0; i < size; i++) c->h_id2offset[order[i]] = (uint32_t)i;
+  c->vocab_size = size;
+  c->train_words = tw;
+  std::vector<long long> cn(size);
+  for (long long i = 0; i < size; i++) cn[i] = c->h_deg[order[i]];
+  // unigram table (word2vec.cu:674-694)
+  std::vector<int32_t> table(kTableSize);
+  {
+    double twp = 0, d1, power = 0.75;
+    long long i = 0;
+    for (long long a = 0; a < size; a++) twp += pow((double)cn[a], power);
+    d1 = pow((double)cn[0], power) / twp;
+    for (int64_t a = 0; a < kTableSize; a++) {
+      table[a] = (int32_t)i;
+      if (a / (double)kTableSize > d1) {
+        i++;
+        d1 += pow((double)cn[i < size ? i : size - 1], power) / twp;
+      }
+      if (i >= size) i = size - 1;
+    }
+  }
+  // subsampling thresholds (word2vec.cu:180-212)
+  std::vector<uint16_t> thr;
+  {
+    double sample = c->o.sample;
+    if (sample > 0.0 && tw > 0) {
+      double stw = sample * (double)tw;
+      if (stw > 0.0) {
+        thr.assign(size, 65535);
+        for (long long i = 0; i < size; i++) {
+          long long count = cn[i];
+          if (count <= 0) continue;
+          double prob = (sqrt(count / stw) + 1.0) * (stw / (double)count);
+          if (prob > 1.0) prob = 1.0;
+          else if (prob < 0.0) prob = 0.0;
+          thr[i] = prob >= 1.0 ? 65535 : (uint16_t)(prob * 65535.0 + 0.5);
+        }
+      }
+    }
+  }
+  // exp table (word2vec.cu:2292-2297), host libm
+  float et[1000];
+  for (int i = 0; i < 1000; i++) {
+    et[i] = expf((i / (float)1000 * 2 - 1) * 6);
+    et[i] = et[i] / (et[i] + 1);
+  }
+  CK(c->id2offset.ensure(V), "init_model");
+  CK(cudaMemcpy(c->id2offset.p, c->h_id2offset.data(), 4 * (size_t)V, cudaMemcpyHostToDevice), "init_model");
+  CK(c->table.ensure(kTableSize), "init_model: unigram table");
+  CK(cudaMemcpy(c->table.p, table.data(), 4 * (size_t)kTableSize, cudaMemcpyHostToDevice), "init_model");
+  c->use_thr = !thr.empty();
+  CK(c->thr.ensure(std::max<size_t>(thr.size(), 1)), "init_model");
+  if (c->use_thr) CK(cudaMemcpy(c->thr.p, thr.data(), 2 * thr.size(), cudaMemcpyHostToDevice), "init_model");
+  CK(c->exp_table.ensure(1000), "init_model");
+  CK(cudaMemcpy(c->exp_table.p, et, sizeof et, cudaMemcpyHostToDevice), "init_model");
+  const uint64_t nel = (uint64_t)size * dim;
+  CK(c->syn0.ensure(nel), "init_model: syn0");
+  CK(c->syn1.ensure(nel), "init_model: syn1");
+  CK(cudaMemsetAsync(c->syn1.p, 0, 4 * nel, c->stream), "init_model");
+  k_init_syn0<<<grid_for(c, nel, 256), 256, 0, c->stream>>>(c->syn0.p, (uint64_t)size, dim, c->jump.p);
+  c->launches++;
+  CK(cudaGetLastError(), "init_model");
+  CK(c->sim.ensure(V), "init_model");
+  CK(cudaMemsetAsync(c->sim.p, 0, 4 * (size_t)V, c->stream), "init_model");
+  CK(cudaStreamSynchronize(c->stream), "init_model");
+  c->model_ready = true;
+  return FELOG_OK;
+}
+
+extern "C" felog_status felog_vocab_info(felog_ctx *c, uint64_t *vocab_size, uint64_t *train_words) {
+  if (!c) return FELOG_INVALID_ARG;
+  if (!c->model_ready) return fail(c, FELOG_NOT_READY, "model not initialised");
+  if (vocab_size) *vocab_size = (uint64_t)c->vocab_size;
+  if (train_words) *train_words = (uint64_t)c->train_words;
+  return FELOG_OK;
+}
+
+extern "C" felog_status felog_get_vocab(felog_ctx *c, uint32_t *vocab_vertex, uint32_t *id2offset) {
+  if (!c) return FELOG_INVALID_ARG;
+  if (!c->model_ready) return fail(c, FELOG_NOT_READY, "model not initialised");
+  if (vocab_vertex) memcpy(vocab_vertex, c->h_vocab_vertex.data(), 4 * c->h_vocab_vertex.size());
+  if (id2offset) memcpy(id2offset, c->h_id2offset.data(), 4 * c->h_id2offset.size());
+  return FELOG_OK;
+}
+
+namespace {
+
+float schedule_alpha(const felog_ctx *c, uint32_t round) {
+  // ExponentialDecayLR(0.025, 0.1), lr_scheduler.hpp:23-31: step counts rounds from 0
+  float initial = c->o.use_cli_alpha ? c->o.alpha : 0.025f;
+  float decay = 0.1f;
+  return initial * expf(-decay * (int)round);
+}
+
+felog_status plan_round(felog_ctx *c, float *ms) {
+  const uint64_t n = c->n_sent;
+  CK(c->p_cand.ensure(n + 1), "plan");
+  CK(c->p_draws.ensure(n + 1), "plan");
+  CK(c->p_cons.ensure(n + 1), "plan");
+  CK(c->p_kept.ensure(n + 1), "plan");
+  CK(c->p_blk.ensure(n + 1), "plan");
+  CK(c->p_state.ensure(n + 1), "plan");
+  CK(c->p_out_off.ensure(n + 1), "plan");
+  CK(c->p_batch_first.ensure(n + 2), "plan");
+  CK(c->p_neg_state.ensure(n + 1), "plan");
+  CK(c->p_negs.ensure(n * (uint64_t)c->o.negative + 1), "plan");
+  PlanArgs a{};
+  a.arena = c->arena.p;
+  a.sent_ptr = c->sent_ptr.p;
+  a.sent_len = c->sent_len.p;
+  a.n_sent = n;
+  a.id2offset = c->id2offset.p;
+  a.thr = c->use_thr ? c->thr.p : nullptr;
+  a.table = c->table.p;
+  a.table_size = kTableSize;
+  a.vocab_size = c->vocab_size;
+  a.negative = c->o.negative;
+  a.seed = 0x9E3779B97F4A7C15ULL ^ ((0ULL + 1ULL) << 1) ^ 0x2ULL;  // InitSeedForRank(0, 2), word2vec.cu:146-152
+  a.cand = c->p_cand.p;
+  a.draws = c->p_draws.p;
+  a.considered = c->p_cons.p;
+  a.kept = c->p_kept.p;
+  a.state = c->p_state.p;
+  a.blk = c->p_blk.p;
+  a.out_off = c->p_out_off.p;
+  a.batch_first = c->p_batch_first.p;
+  a.neg_state = c->p_neg_state.p;
+  a.max_batches = n + 1;
+  a.counters = c->counters.p + 4;
+  a.jump = c->jump.p;
+  a.err = c->derr.p;
+  CK(cudaEventRecord(c->ev0, c->stream), "plan");
+  k_plan_scan<<<grid_for(c, n, 256), 256, 0, c->stream>>>(a);
+  c->launches++;
+  k_plan_batches<1024><<<1, 1024, 0, c->stream>>>(a);
+  c->launches++;
+  // out_off = exclusive scan of kept
+  size_t tmp = 0;
+  CK(cub::DeviceScan::ExclusiveSum(nullptr, tmp, c->p_kept.p, c->p_out_off.p, (int)(n + 1), c->stream), "plan");
+  CK(c->cub_tmp.ensure(tmp), "plan");
+  CK(cudaMemsetAsync(c->p_kept.p + n, 0, 4, c->stream), "plan");
+  CK(cub::DeviceScan::ExclusiveSum(c->cub_tmp.p, tmp, c->p_kept.p, c->p_out_off.p, (int)(n + 1), c->stream),
+     "plan");
+  uint64_t total = 0, nb = 0;
+  CK(cudaMemcpyAsync(&total, c->p_out_off.p + n, 8, cudaMemcpyDeviceToHost, c->stream), "plan");
+  unsigned long long hc[2];
+  CK(cudaMemcpyAsync(hc, c->counters.p + 4, sizeof hc, cudaMemcpyDeviceToHost, c->stream), "plan");
+  CK(cudaStreamSynchronize(c->stream), "plan");
+  nb = hc[0];
+  CK(c->p_sen.ensure(total + 1), "plan");
+  a.sen = c->p_sen.p;
+  a.negs = c->p_negs.p;
+  k_plan_emit<<<grid_for(c, n, 256), 256, 0, c->stream>>>(a);
+  c->launches++;
+  if (n) k_plan_negs<<<grid_for(c, n * (uint64_t)c->o.negative, 256), 256, 0, c->stream>>>(a, nb);
+  c->launches++;
+  CK(cudaGetLastError(), "plan");
+  CK(cudaEventRecord(c->ev1, c->stream), "plan");
+  felog_status s = check_dev_err(c, "plan");
+  if (s != FELOG_OK) return s;
+  CK(cudaEventElapsedTime(ms, c->ev0, c->ev1), "plan");
+  c->plan_sent = n;
+  c->plan_sen = total;
+  c->plan_batches = nb;
+  return FELOG_OK;
+}
+
+}  // namespace
+
+extern "C" felog_status felog_train_round(felog_ctx *c, uint32_t round, float alpha, felog_train_stats *stats) {
+  if (!c) return FELOG_INVALID_ARG;
+  if (!c->model_ready) return fail(c, FELOG_NOT_READY, "model not initialised");
+  if (!c->corpus_ready) return fail(c, FELOG_NOT_READY, "no corpus");
+  if (c->o.cbow) return fail(c, FELOG_INVALID_ARG, "-cbow 1 training is not available in this build");
+  if (c->o.reuse_neg) return fail(c, FELOG_INVALID_ARG, "-reuse-neg 1 training is not available in this build");
+  CK(cudaSetDevice(c->device), "train_round");
+  if (alpha < 0) alpha = schedule_alpha(c, round);
+  float ms_plan = 0, ms_train = 0;
+  CK(cudaMemsetAsync(c->counters.p, 0, sizeof(unsigned long long) * 16, c->stream), "train_round");
+  CK(cudaMemsetAsync(c->derr.p, 0, sizeof(int), c->stream), "train_round");
+  felog_status s = plan_round(c, &ms_plan);
+  if (s != FELOG_OK) return s;
+  CK(cudaMemsetAsync(c->counters.p, 0, sizeof(unsigned long long) * 4, c->stream), "train_round");
+  SgArgs g{};
+  g.syn0 = c->syn0.p;
+  g.syn1 = c->syn1.p;
+  g.sen = c->p_sen.p;
+  g.sent_start = c->p_out_off.p;
+  g.blk = c->p_blk.p;
+  g.negs = c->p_negs.p;
+  g.n_sent = c->plan_sent;
+  g.table = c->table.p;
+  g.table_size = kTableSize;
+  g.vocab_size = c->vocab_size;
+  g.exp_table = c->exp_table.p;
+  g.window = c->o.window;
+  g.negative = c->o.negative;
+  g.alpha = alpha;
+  g.next_sent = c->counters.p + 0;
+  g.pairs = c->counters.p + 1;
+  const int blocks = c->o.deterministic ? 1 : c->sm_count * 8;
+  const int threads = c->o.deterministic ? 32 : 256;
+  CK(cudaEventRecord(c->ev0, c->stream), "train_round");
+  switch (c->o.size) {
+    case 32: k_sgns_skipgram<32><<<blocks, threads, 0, c->stream>>>(g); break;
+    case 64: k_sgns_skipgram<64><<<blocks, threads, 0, c->stream>>>(g); break;
+    case 128: k_sgns_skipgram<128><<<blocks, threads, 0, c->stream>>>(g); break;
+    case 256: k_sgns_skipgram<256><<<blocks, threads, 0, c->stream>>>(g); break;
+  }
+  c->launches++;
+  CK(cudaGetLastError(), "train_round: launch");
+  CK(cudaEventRecord(c->ev1, c->stream), "train_round");
+  unsigned long long h[4];
+  CK(cudaMemcpyAsync(h, c->counters.p, sizeof h, cudaMemcpyDeviceToHost, c->stream), "train_round");
+  s = check_dev_err(c, "train_round");
+  if (s != FELOG_OK) return s;
+  CK(cudaEventElapsedTime(&ms_train, c->ev0, c->ev1), "train_round");
+  if (stats) {
+    memset(stats, 0, sizeof(*stats));
+    // words considered = sum of considered tokens per sentence
+    std::vector<uint32_t> cons(c->plan_sent);
+    if (c->plan_sent)
+      CK(cudaMemcpy(cons.data(), c->p_cons.p, 4 * c->plan_sent, cudaMemcpyDeviceToHost), "train_round");
+    uint64_t w = 0;
+    for (uint32_t x : cons) w += x;
+    stats->words = w;
+    stats->kept_words = c->plan_sen;
+    stats->pairs = h[1];
+    stats->sentences = c->plan_sent;
+    stats->batches = c->plan_batches;
+    stats->alpha = alpha;
+    stats->ms_plan = ms_plan;
+    stats->ms_train = ms_train;
+  }
+  return FELOG_OK;
+}
+
+extern "C" felog_status felog_plan_size(felog_ctx *c, uint64_t *n_sentences, uint64_t *n_sen, uint64_t *n_batches) {
+  if (!c) return FELOG_INVALID_ARG;
+  if (n_sentences) *n_sentences = c->plan_sent;
+  if (n_sen) *n_sen = c->plan_sen;
+  if (n_batches) *n_batches = c->plan_batches;
+  return FELOG_OK;
+}
+
+extern "C" felog_status felog_get_plan(felog_ctx *c, int32_t *sen, uint64_t *sent_start, uint64_t *batch_first,
+                                       int32_t *negs) {
+  if (!c) return FELOG_INVALID_ARG;
+  if (sen && c->plan_sen) CK(cudaMemcpy(sen, c->p_sen.p, 4 * c->plan_sen, cudaMemcpyDeviceToHost), "get_plan");
+  if (sent_start)
+    CK(cudaMemcpy(sent_start, c->p_out_off.p, 8 * (c->plan_sent + 1), cudaMemcpyDeviceToHost), "get_plan");
+  if (batch_first)
+    CK(cudaMemcpy(batch_first, c->p_batch_first.p, 8 * (c->plan_batches + 1), cudaMemcpyDeviceToHost), "get_plan");
+  if (negs && c->plan_sent)
+    CK(cudaMemcpy(negs, c->p_negs.p, 4 * c->plan_sent * (uint64_t)c->o.negative, cudaMemcpyDeviceToHost),
+       "get_plan");
+  return FELOG_OK;
+}
+
+namespace {
+
+// interleaved rows -> logical order (see sgns.cuh)
+__global__ void k_unpermute(const float *src, float *dst, uint64_t rows, int dim) {
+  const int Jn = dim / 32;
+  const uint64_t n = rows * (uint64_t)dim;
+  for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < n; e += (uint64_t)gridDim.x * blockDim.x) {
+    uint64_t r = e / dim;
+    int l = (int)(e % dim);
+    dst[e] = src[r * dim + (uint64_t)(l % 32) * Jn + l / 32];
+  }
+}
+
+}  // namespace
+
+extern "C" felog_status felog_get_embeddings(felog_ctx *c, float *syn0, float *syn1, uint64_t cap_floats) {
+  if (!c) return FELOG_INVALID_ARG;
+  if (!c->model_ready) return fail(c, FELOG_NOT_READY, "model not initialised");
+  const int dim = c->o.size;
+  const uint64_t nel = (uint64_t)c->vocab_size * dim;
+  if (cap_floats < nel) return fail(c, FELOG_INVALID_ARG, "get_embeddings: need %llu floats", (unsigned long long)nel);
+  CK(cudaSetDevice(c->device), "get_embeddings");
+  CK(c->out_tmp.ensure(nel), "get_embeddings");
+  for (int which = 0; which < 2; which++) {
+    float *dst = which ? syn1 : syn0;
+    if (!dst) continue;
+    k_unpermute<<<grid_for(c, nel, 256), 256, 0, c->stream>>>(which ? c->syn1.p : c->syn0.p, c->out_tmp.p,
+                                                               (uint64_t)c->vocab_size, dim);
+    c->launches++;
+    CK(cudaGetLastError(), "get_embeddings");
+    CK(cudaMemcpyAsync(dst, c->out_tmp.p, 4 * nel, cudaMemcpyDeviceToHost, c->stream), "get_embeddings");
+    CK(cudaStreamSynchronize(c->stream), "get_embeddings");
+  }
+  return FELOG_OK;
+}
+
+extern "C" uint64_t felog_kernel_launches(const felog_ctx *c) { return c ? c->launches : 0; }
+
+extern "C" felog_status felog_timer_mark(felog_ctx *c, int which) {
+  if (!c || (which != 0 && which != 1)) return FELOG_INVALID_ARG;
+  CK(cudaEventRecord(which ? c->tm1 : c->tm0, c->stream), "timer_mark");
+  return FELOG_OK;
+}
+
+extern "C" felog_status felog_timer_elapsed(felog_ctx *c, float *ms) {
+  if (!c || !ms) return FELOG_INVALID_ARG;
+  CK(cudaEventSynchronize(c->tm1), "timer_elapsed");
+  CK(cudaEventElapsedTime(ms, c->tm0, c->tm1), "timer_elapsed");
+  return FELOG_OK;
+}
+
+extern "C" felog_status felog_set_embeddings(felog_ctx *c, const float *syn0, const float *syn1) {
+  if (!c) return FELOG_INVALID_ARG;
+  if (!c->model_ready) return fail(c, FELOG_NOT_READY, "model not initialised");
+  const int dim = c->o.size;
+  const uint64_t nel = (uint64_t)c->vocab_size * dim;
+  std::vector<float> buf(nel);
+  for (int which = 0; which < 2; which++) {
+    const float *src = which ? syn1 : syn0;
+    if (!src) continue;
+    for (uint64_t r = 0; r < (uint64_t)c->vocab_size; r++)
+      for (int l = 0; l < dim; l++) buf[r * dim + phys_index(dim, l)] = src[r * dim + l];
+    CK(cudaMemcpy(which ? c->syn1.p : c->syn0.p, buf.data(), 4 * nel, cudaMemcpyHostToDevice), "set_embeddings");
+  }
+  return FELOG_OK;
+}
+
+// ---------------------------------------------------------------- budget
+
+extern "C" felog_status felog_budget_check(felog_ctx *c, uint32_t round, felog_budget_stats *stats) {
+  if (!c) return FELOG_INVALID_ARG;
+  if (!c->model_ready) return fail(c, FELOG_NOT_READY, "model not initialised");
+  CK(cudaSetDevice(c->device), "budget_check");
+  CK(cudaMemsetAsync(c->counters.p, 0, sizeof(unsigned long long) * 4, c->stream), "budget_check");
+  ConvArgs a{};
+  a.syn0 = c->syn0.p;
+  a.id2offset = c->id2offset.p;
+  a.row_ptr = c->row_ptr.p;
+  a.adj = c->adj.p;
+  a.v_num = c->V;
+  a.stop = c->stop.p;
+  a.sim = c->sim.p;
+  a.seed = c->o.seed;
+  a.round = round;
+  a.counters = c->counters.p;
+  CK(cudaEventRecord(c->ev0, c->stream), "budget_check");
+  const int blocks = grid_for(c, (uint64_t)c->V * 32, 256, 8);
+  switch (c->o.size) {
+    case 32: k_converge<32><<<blocks, 256, 0, c->stream>>>(a); break;
+    case 64: k_converge<64><<<blocks, 256, 0, c->stream>>>(a); break;
+    case 128: k_converge<128><<<blocks, 256, 0, c->stream>>>(a); break;
+    case 256: k_converge<256><<<blocks, 256, 0, c->stream>>>(a); break;
+  }
+  c->launches++;
+  k_count_stopped<<<grid_for(c, c->V, 256), 256, 0, c->stream>>>(c->stop.p, c->V, c->counters.p + 2);
+  c->launches++;
+  CK(cudaGetLastError(), "budget_check");
+  CK(cudaEventRecord(c->ev1, c->stream), "budget_check");
+  unsigned long long h[4];
+  CK(cudaMemcpyAsync(h, c->counters.p, sizeof h, cudaMemcpyDeviceToHost, c->stream), "budget_check");
+  CK(cudaStreamSynchronize(c->stream), "budget_check");
+  float ms = 0;
+  CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1), "budget_check");
+  // eva_num ratio test (word2vec.cu:2073-2080); the first comparison is against vocab_size
+  uint64_t last = c->have_last_eva ? c->last_eva : (uint64_t)c->vocab_size;
+  float ratio = last ? (float)h[1] / (float)last : 0.0f;
+  int stop_all = (last != 0 && ratio > 0.7f) ? 1 : 0;
+  c->last_eva = h[1];
+  c->have_last_eva = true;
+  if (stats) {
+    memset(stats, 0, sizeof(*stats));
+    stats->evaluated = h[0];
+    stats->unconverged = h[1];
+    stats->stopped_total = h[2];
+    stats->stop_all = stop_all;
+    stats->ms = ms;
+  }
+  return FELOG_OK;
+}
+
+extern "C" felog_status felog_get_similarity(felog_ctx *c, float *sim) {
+  if (!c || !sim) return FELOG_INVALID_ARG;
+  if (!c->model_ready) return fail(c, FELOG_NOT_READY, "model not initialised");
+  CK(cudaMemcpy(sim, c->sim.p, 4 * (size_t)c->V, cudaMemcpyDeviceToHost), "get_similarity");
+  return FELOG_OK;
+}
+
+// ------------------------------------------------------------ whole loop
+
+extern "C" felog_status felog_run(felog_ctx *c, felog_run_stats *st) {
+  if (!c) return FELOG_INVALID_ARG;
+  if (!c->V) return fail(c, FELOG_NOT_READY, "no graph loaded");
+  felog_run_stats rs{};
+  felog_status s;
+  if (!c->model_ready) {
+    s = felog_init_model(c);
+    if (s != FELOG_OK) return s;
+  }
+  const uint32_t min_r = c->o.min_rounds ? c->o.min_rounds : 1;
+  for (uint32_t r = 0;; r++) {
+    if (c->o.max_rounds > 0 && (int)r >= c->o.max_rounds) break;
+    felog_walk_stats ws;
+    s = felog_walk_round(c, r, nullptr, &ws);
+    if (s != FELOG_OK) return s;
+    felog_train_stats ts;
+    s = felog_train_round(c, r, -1.0f, &ts);
+    if (s != FELOG_OK) return s;
+    rs.rounds = r + 1;
+    rs.walk_tokens += ws.n_tokens;
+    rs.train_words += ts.words;
+    rs.walk_ms += ws.ms;
+    rs.train_ms += ts.ms_plan + ts.ms_train;
+    if (r + 1 >= min_r) {  // train_iter >= init_round, word2vec.cu:2011-2017
+      felog_budget_stats bs;
+      s = felog_budget_check(c, r, &bs);
+      if (s != FELOG_OK) return s;
+      rs.budget_ms += bs.ms;
+      rs.final_unconverged = bs.unconverged;
+      if (bs.stop_all) break;
+    }
+  }
+  rs.total_ms = rs.walk_ms + rs.train_ms + rs.budget_ms;
+  if (st) *st = rs;
+  return FELOG_OK;
+}
+
+extern "C" felog_status felog_write_embeddings(felog_ctx *c, const char *path) {
+  if (!c || !path) return FELOG_INVALID_ARG;
+  if (!c->model_ready) return fail(c, FELOG_NOT_READY, "model not initialised");
+  const int dim = c->o.size;
+  std::vector<float> s0((uint64_t)c->vocab_size * dim);
+  felog_status s = felog_get_embeddings(c, s0.data(), nullptr, s0.size());
+  if (s != FELOG_OK) return s;
+  FILE *fo = fopen(path, "wb");
+  if (!fo) return fail(c, FELOG_IO_ERROR, "cannot open %s", path);
+  // word2vec.cu:2121-2127
+  fprintf(fo, "%lld %lld\n", (long long)c->vocab_size, (long long)dim);
+  for (long long a = 0; a < c->vocab_size; a++) {
+    fprintf(fo, "%u ", c->h_vocab_vertex[a]);
+    if (c->o.binary) {
+      fwrite(&s0[(uint64_t)a * dim], sizeof(float), dim, fo);
+    } else {
+      for (int b = 0; b < dim; b++) fprintf(fo, "%lf ", s0[(uint64_t)a * dim + b]);
+    }
+    fprintf(fo, "\n");
+  }
+  if (fclose(fo) != 0) return fail(c, FELOG_IO_ERROR, "write failed on %s", path);
+  return FELOG_OK;
+}

@@ -1,0 +1,201 @@
+// Skip-gram negative-sampling kernels.
+//
+// One warp per sentence (Hogwild across warps, like the reference's one block
+// per sentence).  Row layout is interleaved: for a row of DIM = 32 * J floats,
+// physical position lane * J + j holds logical dimension lane + 32 j, so each
+// lane moves its J values with one vector load / one vector reduction and the
+// dot product below sums the products in exactly the order of the reference's
+// shared-memory tree (word2vec.cu:510-518: pair t with t + DIM/2 via a*b + c,
+// then halve).  Every multiply-add that the reference kernel fuses is written
+// as an explicit fmaf and every other operation as a rounded intrinsic, so a
+// single warp reproduces the reference's sequential semantics bit for bit.
+#pragma once
+
+#include "common.cuh"
+
+namespace felog {
+
+constexpr int kMaxNeg = 15;
+constexpr int kChunk = 8;  // targets whose rows are loaded together
+
+struct SgArgs {
+  float *syn0;
+  float *syn1;
+  const int32_t *sen;
+  const uint64_t *sent_start;  // n_sent + 1
+  const uint32_t *blk;         // index of the sentence in its batch
+  const int32_t *negs;         // reuse-neg: negative per sentence (sentence-major)
+  uint64_t n_sent;
+  const int32_t *table;
+  uint64_t table_size;
+  long long vocab_size;
+  const float *exp_table;
+  int window;
+  int negative;
+  float alpha;
+  unsigned long long *next_sent;
+  unsigned long long *pairs;
+};
+
+template <int J>
+__device__ __forceinline__ void ld_row(const float *row, float (&r)[J]) {
+  const float *p = row + lane_id() * J;
+  if constexpr (J == 8) {
+    float4 u = __ldcg(reinterpret_cast<const float4 *>(p));
+    float4 v = __ldcg(reinterpret_cast<const float4 *>(p) + 1);
+    r[0] = u.x; r[1] = u.y; r[2] = u.z; r[3] = u.w; r[4] = v.x; r[5] = v.y; r[6] = v.z; r[7] = v.w;
+  } else if constexpr (J == 4) {
+    float4 u = __ldcg(reinterpret_cast<const float4 *>(p));
+    r[0] = u.x; r[1] = u.y; r[2] = u.z; r[3] = u.w;
+  } else if constexpr (J == 2) {
+    float2 u = __ldcg(reinterpret_cast<const float2 *>(p));
+    r[0] = u.x; r[1] = u.y;
+  } else {
+    r[0] = __ldcg(p);
+  }
+}
+
+__device__ __forceinline__ void red_add_v4(float *p, float a, float b, float c, float d) {
+  asm volatile("red.relaxed.gpu.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(p), "f"(a), "f"(b), "f"(c),
+               "f"(d)
+               : "memory");
+}
+__device__ __forceinline__ void red_add_v2(float *p, float a, float b) {
+  asm volatile("red.relaxed.gpu.global.add.v2.f32 [%0], {%1, %2};" ::"l"(p), "f"(a), "f"(b) : "memory");
+}
+
+template <int J>
+__device__ __forceinline__ void red_row(float *row, const float (&u)[J]) {
+  float *p = row + lane_id() * J;
+  if constexpr (J == 8) {
+    red_add_v4(p, u[0], u[1], u[2], u[3]);
+    red_add_v4(p + 4, u[4], u[5], u[6], u[7]);
+  } else if constexpr (J == 4) {
+    red_add_v4(p, u[0], u[1], u[2], u[3]);
+  } else if constexpr (J == 2) {
+    red_add_v2(p, u[0], u[1]);
+  } else {
+    atomicAdd(p, u[0]);
+  }
+}
+
+// dot product in the reference tree order (FSIZE = DIM / 2)
+template <int J>
+__device__ __forceinline__ float sg_dot(const float (&x)[J], const float (&y)[J]) {
+  if constexpr (J == 1) {
+    float xs = __shfl_down_sync(0xffffffffu, x[0], 16);
+    float ys = __shfl_down_sync(0xffffffffu, y[0], 16);
+    float s = __fmaf_rn(xs, ys, __fmul_rn(x[0], y[0]));  // meaningful in lanes 0..15
+#pragma unroll
+    for (int o = 8; o > 0; o >>= 1) s = __fadd_rn(s, __shfl_xor_sync(0xffffffffu, s, o));
+    return __shfl_sync(0xffffffffu, s, 0);
+  } else {
+    float s[J / 2];
+#pragma unroll
+    for (int j = 0; j < J / 2; j++) s[j] = __fmaf_rn(x[j + J / 2], y[j + J / 2], __fmul_rn(x[j], y[j]));
+#pragma unroll
+    for (int h = J / 4; h >= 1; h >>= 1)
+#pragma unroll
+      for (int j = 0; j < h; j++) s[j] = __fadd_rn(s[j], s[j + h]);
+    float r = s[0];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) r = __fadd_rn(r, __shfl_xor_sync(0xffffffffu, r, o));
+    return r;
+  }
+}
+
+// g = (label - sigma(f)) * alpha with the reference's quantized sigmoid
+// (word2vec.cu:519-526; index (f + 6) * 83, EXP_TABLE_SIZE / MAX_EXP / 2 = 83).
+__device__ __forceinline__ float sg_grad(float f, int label, const float *s_exp, float alpha) {
+  if (f > 6.0f) return __fmul_rn((float)(label - 1), alpha);
+  if (f < -6.0f) return __fmul_rn((float)label, alpha);
+  int idx = (int)__fmul_rn(__fadd_rn(f, 6.0f), 83.0f);
+  return __fmul_rn(__fsub_rn((float)label, s_exp[idx]), alpha);
+}
+
+// skip_gram_kernel semantics (word2vec.cu:442-536, hs = 0) per warp.
+template <int DIM>
+__global__ void __launch_bounds__(256) k_sgns_skipgram(SgArgs a) {
+  constexpr int J = DIM / 32;
+  __shared__ float s_exp[1000];
+  for (int i = threadIdx.x; i < 1000; i += blockDim.x) s_exp[i] = a.exp_table[i];
+  __syncthreads();
+  const int lane = lane_id();
+  unsigned long long my_pairs = 0;
+  for (;;) {
+    unsigned long long s = 0;
+    if (lane == 0) s = atomicAdd(a.next_sent, 1ULL);
+    s = __shfl_sync(0xffffffffu, s, 0);
+    if (s >= a.n_sent) break;
+    const long long sb = (long long)a.sent_start[s], se = (long long)a.sent_start[s + 1];
+    unsigned long long nr = a.blk[s];
+    for (long long pos = sb; pos < se; pos++) {
+      const int word = a.sen[pos];
+      nr = nr * 2514903917ULL + 11ULL;  // the reference's window LCG (word2vec.cu:458)
+      const int b = (int)(nr % (unsigned long long)a.window);
+      for (int aa = b; aa < a.window * 2 + 1 - b; aa++) {
+        if (aa == a.window) continue;
+        const long long c = pos - a.window + aa;
+        if (c < sb || c >= se) continue;
+        const int l1 = a.sen[c];
+        float *xrow = a.syn0 + (long long)l1 * DIM;
+        float x[J];
+        ld_row<J>(xrow, x);
+        float neu[J];
+#pragma unroll
+        for (int j = 0; j < J; j++) neu[j] = 0.0f;
+        my_pairs++;
+        for (int d0 = 0; d0 <= a.negative; d0 += kChunk) {
+          int tg[kChunk];
+          int lab[kChunk];
+          float y[kChunk][J];
+          const int nd = min(kChunk, a.negative + 1 - d0);
+          // targets of this chunk, in the reference's draw order
+#pragma unroll
+          for (int q = 0; q < kChunk; q++) {
+            tg[q] = -1;
+            if (q < nd) {
+              const int d = d0 + q;
+              if (d == 0) {
+                tg[q] = word;
+                lab[q] = 1;
+              } else {
+                nr = nr * 25214903917ULL + 11ULL;
+                int t = a.table[(nr >> 16) % a.table_size];
+                if (t == 0) t = (int)(nr % (unsigned long long)(a.vocab_size - 1) + 1);
+                tg[q] = t == word ? -1 : t;
+                lab[q] = 0;
+              }
+            }
+          }
+#pragma unroll
+          for (int q = 0; q < kChunk; q++)
+            if (tg[q] >= 0) ld_row<J>(a.syn1 + (long long)tg[q] * DIM, y[q]);
+#pragma unroll
+          for (int q = 0; q < kChunk; q++) {
+            if (tg[q] < 0) continue;
+            const float f = sg_dot<J>(x, y[q]);
+            const float g = sg_grad(f, lab[q], s_exp, a.alpha);
+            float upd[J];
+#pragma unroll
+            for (int j = 0; j < J; j++) {
+              neu[j] = __fmaf_rn(g, y[q][j], neu[j]);
+              upd[j] = __fmul_rn(g, x[j]);
+            }
+            red_row<J>(a.syn1 + (long long)tg[q] * DIM, upd);
+            // a later target with the same row sees this update
+#pragma unroll
+            for (int r = q + 1; r < kChunk; r++)
+              if (tg[r] == tg[q])
+#pragma unroll
+                for (int j = 0; j < J; j++) y[r][j] = __fadd_rn(y[q][j], upd[j]);
+          }
+        }
+        red_row<J>(xrow, neu);
+      }
+    }
+  }
+  if (lane == 0 && my_pairs) atomicAdd(a.pairs, my_pairs);
+}
+
+}  // namespace felog

@@ -176,6 +176,7 @@ int orc_walk_round(const orc_csr *g, uint32_t walker_num, const uint8_t *stop_fl
       }
       iter++;
       st->n_iterations++;
+      if (iter > (1u << 24)) return -3; /* same limit as the device walker */
       if (deg == 2 && g->nbr[b] == cur) break;               /* walk.hpp:977-979 */
       uint64_t cand = b + r;
       if (step == 0 && g->nbr[cand] == cur) continue;        /* walk.hpp:981-983 */
@@ -616,6 +617,7 @@ uint64_t orc_convergence(const float *syn0, const uint32_t *id2offset, int dim, 
   uint32_t chosen[30];
   for (uint32_t v = 0; v < g->v_num; v++) {
     if (stop_flags[v]) continue; /* word2vec.cu:2023-2027 */
+    if (id2offset[v] == 0xFFFFFFFFu) continue; /* no row (out of vocabulary) */
     uint64_t b = g->row_ptr[v];
     uint32_t deg = (uint32_t)(g->row_ptr[v + 1] - b);
     int n = deg;
@@ -628,12 +630,15 @@ uint64_t orc_convergence(const float *syn0, const uint32_t *id2offset, int dim, 
     float s = 0.0f;
     if (n > 0) {
       float sum = 0.0f;
+      int used = 0;
       const float *a = syn0 + (uint64_t)id2offset[v] * dim;
       for (int j = 0; j < n; j++) {
         uint32_t u = g->nbr[b + chosen[j]];
+        if (id2offset[u] == 0xFFFFFFFFu) continue;
         sum += orc_cosine(a, syn0 + (uint64_t)id2offset[u] * dim, dim);
+        used++;
       }
-      s = sum / n;
+      s = used > 0 ? sum / used : 0.0f;
     }
     if (sim) sim[v] = s;
     if (s > 0.65) stop_flags[v] = 1; /* word2vec.cu:2056-2061 */

@@ -1,0 +1,69 @@
+"""Walk-budget (per-vertex convergence) parity and the whole round loop."""
+import numpy as np
+import pytest
+
+import felog_b200 as fb
+import oracle_binding as ob
+from conftest import load_golden
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("dim", [64, 128])
+def test_convergence_check_matches_oracle(dim):
+    fx = load_golden("walk_rmat4096.npz")
+    e, V = fx["edges"], int(fx["V"])
+    f = fb.Felog(v_num=V, size=dim, window=10, negative=5, cbow=0, reuse_neg=0, min_count=0, seed=99)
+    f.load_graph(e, V)
+    f.init_model()
+    for r in range(3):
+        f.walk_round(r)
+        f.train_round(r)
+    s0, _ = f.embeddings()
+    vv, id2, vs, _ = f.vocab()
+    flags0 = np.zeros(V, np.uint8)
+    flags0[::17] = 1  # already converged vertices are not re-evaluated
+    f.set_stop_flags(flags0)
+    st = f.budget_check(5)
+    c = ob.OracleCsr(e, V)
+    eva, oflags, osim = ob.convergence(s0, id2, dim, c, flags0, f.opts.seed, 5)
+    np.testing.assert_array_equal(f.stop_flags(), oflags)
+    sim = f.similarity()
+    ev = flags0 == 0
+    np.testing.assert_array_equal(sim[ev], osim[ev])
+    assert st["unconverged"] == eva and st["evaluated"] == int(ev.sum())
+    assert st["stopped_total"] == int(oflags.sum())
+
+
+def test_run_loop_terminates_and_writes_reference_format(tmp_path):
+    g = fb.synth_graph(seed=3, v_target=4096, e_target=32768, holdout=0.1)
+    V = g["v_num"]
+    f = fb.Felog(v_num=V, size=128, window=10, negative=5, cbow=0, reuse_neg=0, min_count=0, min_rounds=2,
+                 max_rounds=12, seed=3)
+    f.load_graph(g["edges"], V)
+    rs = f.run()
+    assert 2 <= rs["rounds"] <= 12 and rs["walk_tokens"] > 0 and rs["train_words"] > 0
+    p = str(tmp_path / "emb.txt")
+    f.write_embeddings(p)
+    lines = open(p).read().splitlines()
+    assert lines[0] == f"{V} 128"  # "%lld %lld\n" (word2vec.cu:2121)
+    vv, id2, vs, _ = f.vocab()
+    s0, _ = f.embeddings()
+    first = lines[1].split(" ")
+    assert first[0] == str(vv[0]) and first[-1] == "" and len(first) == 130  # "%s " + 128 x "%lf " (:2123-2125)
+    assert first[1] == "%lf" % s0[0]
+    assert len(lines) == V + 1
+
+
+def test_stopped_vertices_spawn_no_walkers():
+    fx = load_golden("walk_rmat512.npz")
+    V = int(fx["V"])
+    f = fb.Felog(v_num=V, seed=1)
+    f.load_graph(fx["edges"], V)
+    flags = np.zeros(V, np.uint8)
+    flags[: V // 2] = 1
+    f.set_stop_flags(flags)
+    st = f.walk_round(0)
+    tok, off = f.corpus()
+    assert st["n_sentences"] == V - V // 2
+    assert (tok[off[:-1].astype(np.int64)] >= V // 2).all()
