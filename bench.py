@@ -40,6 +40,9 @@ CONFIGS = {
     "c2": dict(workload="plain FP32, seed-1 R-MAT 2,238,731 vertex ids / 34.7M undirected edges, 5% held out",
                seed=1, v_target=2238731, e_target=34_700_000, abcd=(0.57, 0.19, 0.19, 0.05), lognormal=False,
                holdout=0.05),
+    "prof": dict(workload="profiling case, seed-1 R-MAT 524,288 vertex ids / 8M undirected edges, 5% held out",
+                 seed=1, v_target=524288, e_target=8_000_000, abcd=(0.57, 0.19, 0.19, 0.05), lognormal=False,
+                 holdout=0.05),
     "c1": dict(workload="plain FP32, seed-0 R-MAT 16,384 vertex ids / 131,072 undirected edges, 10% held out",
                seed=0, v_target=16384, e_target=131072, abcd=(0.57, 0.19, 0.19, 0.05), lognormal=False,
                holdout=0.10),

@@ -891,7 +891,6 @@ extern "C" felog_status felog_train_round(felog_ctx *c, uint32_t round, float al
   if (!c) return FELOG_INVALID_ARG;
   if (!c->model_ready) return fail(c, FELOG_NOT_READY, "model not initialised");
   if (!c->corpus_ready) return fail(c, FELOG_NOT_READY, "no corpus");
-  if (c->o.cbow) return fail(c, FELOG_INVALID_ARG, "-cbow 1 training is not available in this build");
   if (c->o.reuse_neg) return fail(c, FELOG_INVALID_ARG, "-reuse-neg 1 training is not available in this build");
   CK(cudaSetDevice(c->device), "train_round");
   if (alpha < 0) alpha = schedule_alpha(c, round);
@@ -921,11 +920,20 @@ extern "C" felog_status felog_train_round(felog_ctx *c, uint32_t round, float al
   const int blocks = c->o.deterministic ? 1 : c->sm_count * 8;
   const int threads = c->o.deterministic ? 32 : 256;
   CK(cudaEventRecord(c->ev0, c->stream), "train_round");
-  switch (c->o.size) {
-    case 32: k_sgns_skipgram<32><<<blocks, threads, 0, c->stream>>>(g); break;
-    case 64: k_sgns_skipgram<64><<<blocks, threads, 0, c->stream>>>(g); break;
-    case 128: k_sgns_skipgram<128><<<blocks, threads, 0, c->stream>>>(g); break;
-    case 256: k_sgns_skipgram<256><<<blocks, threads, 0, c->stream>>>(g); break;
+  if (c->o.cbow) {
+    switch (c->o.size) {
+      case 32: k_sgns_cbow<32><<<blocks, threads, 0, c->stream>>>(g); break;
+      case 64: k_sgns_cbow<64><<<blocks, threads, 0, c->stream>>>(g); break;
+      case 128: k_sgns_cbow<128><<<blocks, threads, 0, c->stream>>>(g); break;
+      case 256: k_sgns_cbow<256><<<blocks, threads, 0, c->stream>>>(g); break;
+    }
+  } else {
+    switch (c->o.size) {
+      case 32: k_sgns_skipgram<32><<<blocks, threads, 0, c->stream>>>(g); break;
+      case 64: k_sgns_skipgram<64><<<blocks, threads, 0, c->stream>>>(g); break;
+      case 128: k_sgns_skipgram<128><<<blocks, threads, 0, c->stream>>>(g); break;
+      case 256: k_sgns_skipgram<256><<<blocks, threads, 0, c->stream>>>(g); break;
+    }
   }
   c->launches++;
   CK(cudaGetLastError(), "train_round: launch");

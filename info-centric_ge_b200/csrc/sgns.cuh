@@ -198,4 +198,100 @@ __global__ void __launch_bounds__(256) k_sgns_skipgram(SgArgs a) {
   if (lane == 0 && my_pairs) atomicAdd(a.pairs, my_pairs);
 }
 
+// cbow_kernel semantics (word2vec.cu:538-646, hs = 0) per warp: the mean of
+// the window's context rows (summed in window order, then divided by the
+// count) is scored against the positive and K negatives; every context row
+// then receives the accumulated error.
+template <int DIM>
+__global__ void __launch_bounds__(256) k_sgns_cbow(SgArgs a) {
+  constexpr int J = DIM / 32;
+  __shared__ float s_exp[1000];
+  for (int i = threadIdx.x; i < 1000; i += blockDim.x) s_exp[i] = a.exp_table[i];
+  __syncthreads();
+  const int lane = lane_id();
+  unsigned long long my_pairs = 0;
+  for (;;) {
+    unsigned long long s = 0;
+    if (lane == 0) s = atomicAdd(a.next_sent, 1ULL);
+    s = __shfl_sync(0xffffffffu, s, 0);
+    if (s >= a.n_sent) break;
+    const long long sb = (long long)a.sent_start[s], se = (long long)a.sent_start[s + 1];
+    unsigned long long nr = a.blk[s];
+    for (long long pos = sb; pos < se; pos++) {
+      const int word = a.sen[pos];
+      nr = nr * 2514903917ULL + 11ULL;
+      const int b = (int)(nr % (unsigned long long)a.window);
+      float neu1[J], neu1e[J];
+#pragma unroll
+      for (int j = 0; j < J; j++) neu1[j] = neu1e[j] = 0.0f;
+      int cw = 0;
+      for (int aa = b; aa < a.window * 2 + 1 - b; aa++) {
+        if (aa == a.window) continue;
+        const long long c = pos - a.window + aa;
+        if (c < sb || c >= se) continue;
+        float x[J];
+        ld_row<J>(a.syn0 + (long long)a.sen[c] * DIM, x);
+#pragma unroll
+        for (int j = 0; j < J; j++) neu1[j] = __fadd_rn(neu1[j], x[j]);
+        cw++;
+      }
+      if (!cw) continue;
+#pragma unroll
+      for (int j = 0; j < J; j++) neu1[j] = __fdiv_rn(neu1[j], (float)cw);
+      my_pairs += cw;
+      for (int d0 = 0; d0 <= a.negative; d0 += kChunk) {
+        int tg[kChunk];
+        int lab[kChunk];
+        float y[kChunk][J];
+        const int nd = min(kChunk, a.negative + 1 - d0);
+#pragma unroll
+        for (int q = 0; q < kChunk; q++) {
+          tg[q] = -1;
+          if (q < nd) {
+            const int d = d0 + q;
+            if (d == 0) {
+              tg[q] = word;
+              lab[q] = 1;
+            } else {
+              nr = nr * 25214903917ULL + 11ULL;
+              int t = a.table[(nr >> 16) % a.table_size];
+              if (t == 0) t = (int)(nr % (unsigned long long)(a.vocab_size - 1) + 1);
+              tg[q] = t == word ? -1 : t;
+              lab[q] = 0;
+            }
+          }
+        }
+#pragma unroll
+        for (int q = 0; q < kChunk; q++)
+          if (tg[q] >= 0) ld_row<J>(a.syn1 + (long long)tg[q] * DIM, y[q]);
+#pragma unroll
+        for (int q = 0; q < kChunk; q++) {
+          if (tg[q] < 0) continue;
+          const float f = sg_dot<J>(neu1, y[q]);
+          const float g = sg_grad(f, lab[q], s_exp, a.alpha);
+          float upd[J];
+#pragma unroll
+          for (int j = 0; j < J; j++) {
+            neu1e[j] = __fmaf_rn(g, y[q][j], neu1e[j]);
+            upd[j] = __fmul_rn(g, neu1[j]);
+          }
+          red_row<J>(a.syn1 + (long long)tg[q] * DIM, upd);
+#pragma unroll
+          for (int r = q + 1; r < kChunk; r++)
+            if (tg[r] == tg[q])
+#pragma unroll
+              for (int j = 0; j < J; j++) y[r][j] = __fadd_rn(y[q][j], upd[j]);
+        }
+      }
+      for (int aa = b; aa < a.window * 2 + 1 - b; aa++) {
+        if (aa == a.window) continue;
+        const long long c = pos - a.window + aa;
+        if (c < sb || c >= se) continue;
+        red_row<J>(a.syn0 + (long long)a.sen[c] * DIM, neu1e);
+      }
+    }
+  }
+  if (lane == 0 && my_pairs) atomicAdd(a.pairs, my_pairs);
+}
+
 }  // namespace felog
