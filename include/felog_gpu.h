@@ -180,6 +180,24 @@ felog_status felog_get_degrees(felog_ctx *ctx, uint32_t *deg);
 felog_status felog_build_alias(felog_ctx *ctx);
 felog_status felog_get_alias(felog_ctx *ctx, float *prob, uint32_t *alias);
 
+/* No counterpart in the reference.  The same alias tables as
+ * felog_build_alias, for callers that cannot allocate device memory (their
+ * device memory belongs to their own allocator, or they must not grow their
+ * footprint after start-up).  It allocates nothing: inputs and outputs are the
+ * caller's device buffers (row_ptr: v_num + 1 u64 CSR offsets; weight, prob,
+ * alias: e_num entries) and its worklists live in a fixed device array of
+ * FELOG_NOALLOC_MAX_ENTRIES entries that every GPU loading this library holds
+ * until exit; larger graphs get FELOG_INVALID_ARG.  The first call on a device
+ * (with that device current) looks the array up; make it before any stream
+ * capture.  Calls share the array, so calls that overlap on the GPU race.
+ * stream: a cudaStream_t, or NULL for the default stream; the call
+ * synchronizes it.  Returns FELOG_INVALID_ARG for a null buffer, for more than
+ * FELOG_NOALLOC_MAX_ENTRIES entries (before touching the device) and for a
+ * negative or non-finite weight; FELOG_CUDA_ERROR when a CUDA call fails. */
+#define FELOG_NOALLOC_MAX_ENTRIES (1ull << 22)
+felog_status felog_build_alias_noalloc(const uint64_t *row_ptr, const float *weight, uint32_t v_num,
+                                       uint64_t e_num, float *prob, uint32_t *alias, void *stream);
+
 /* ---- walk ---- */
 felog_status felog_set_stop_flags(felog_ctx *ctx, const uint8_t *flags);
 felog_status felog_get_stop_flags(felog_ctx *ctx, uint8_t *flags);

@@ -139,6 +139,7 @@ def gpu_lib():
         L.felog_kernel_launches.restype = ctypes.c_uint64
         L.felog_timer_mark.argtypes = [_P, ctypes.c_int]
         L.felog_timer_elapsed.argtypes = [_P, ctypes.POINTER(ctypes.c_float)]
+        L.felog_build_alias_noalloc.argtypes = [_P, _P, ctypes.c_uint32, ctypes.c_uint64, _P, _P, _P]
         _gpu = L
     return _gpu
 
@@ -415,6 +416,16 @@ def synth_graph(seed, v_target, e_target, abcd=(0.57, 0.19, 0.19, 0.05), lognorm
         L.felog_synth_free(h)
     return dict(v_num=int(info.v_num), edges=edges, test_src=ts, test_dst=td, test_label=tl,
                 info=_struct_dict(info))
+
+
+def build_alias_noalloc(row_ptr_dev, weight_dev, v_num, e_num, prob_dev, alias_dev, stream=None):
+    """felog_build_alias_noalloc on caller-owned device buffers (integer device addresses).
+
+    For callers that cannot allocate device memory; raises FelogError on failure."""
+    L = gpu_lib()
+    st = L.felog_build_alias_noalloc(row_ptr_dev, weight_dev, v_num, e_num, prob_dev, alias_dev, stream)
+    if st != 0:
+        raise FelogError(st, "felog_build_alias_noalloc failed (oversized graph, bad weight or CUDA error)")
 
 
 def auc(scores, labels):
