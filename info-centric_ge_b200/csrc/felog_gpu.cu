@@ -96,6 +96,8 @@ struct felog_ctx {
   DevBuf<double> inj_p;
   DevBuf<uint32_t> flags_tmp;
   DevBuf<double> kl_partial;
+  DevBuf<double> corr_tab;
+  bool corr_tab_ready = false;
 
   // vocabulary / model
   long long vocab_size = 0, train_words = 0;
@@ -262,7 +264,7 @@ extern "C" void felog_destroy(felog_ctx *c) {
   c->stop.release(); c->active.release(); c->arena.release(); c->sent_ptr.release(); c->sent_len.release();
   c->visit_freq.release(); c->counters.release(); c->derr.release(); c->inj_idx_off.release();
   c->inj_p_off.release(); c->inj_idx.release(); c->inj_p.release(); c->flags_tmp.release();
-  c->kl_partial.release(); c->id2offset.release(); c->thr.release(); c->table.release();
+  c->kl_partial.release(); c->corr_tab.release(); c->id2offset.release(); c->thr.release(); c->table.release();
   c->exp_table.release(); c->syn0.release(); c->syn1.release(); c->jump.release();
   c->p_cand.release(); c->p_draws.release(); c->p_cons.release(); c->p_kept.release(); c->p_blk.release();
   c->p_state.release(); c->p_neg_state.release(); c->p_out_off.release(); c->p_batch_first.release();
@@ -539,6 +541,13 @@ extern "C" felog_status felog_walk_round(felog_ctx *c, uint32_t round, const fel
       CK(cudaMemcpyAsync(c->inj_p.p, draws->p, 8 * draws->n_p, cudaMemcpyHostToDevice, c->stream),
          "walk_round: draws");
   }
+  if (!c->corr_tab_ready) {
+    CK(c->corr_tab.ensure((kCorrTableS + 1) * (kCorrTableS + 1)), "walk_round: correlation table");
+    k_corr_table<<<64, 256, 0, c->stream>>>(c->corr_tab.p);
+    c->launches++;
+    CK(cudaGetLastError(), "walk_round: correlation table");
+    c->corr_tab_ready = true;
+  }
   CK(cudaMemsetAsync(c->counters.p, 0, sizeof(unsigned long long) * 16, c->stream), "walk_round");
   CK(cudaMemsetAsync(c->derr.p, 0, sizeof(int), c->stream), "walk_round");
   WalkArgs a{};
@@ -566,6 +575,7 @@ extern "C" felog_status felog_walk_round(felog_ctx *c, uint32_t round, const fel
   a.sent_ptr = c->sent_ptr.p;
   a.sent_len = c->sent_len.p;
   a.visit_freq = c->visit_freq.p;
+  a.corr_tab = c->corr_tab.p;
   a.next_walker = reinterpret_cast<unsigned int *>(c->counters.p + 9);
   a.stats = c->counters.p;
   a.err = c->derr.p;
@@ -917,6 +927,8 @@ extern "C" felog_status felog_train_round(felog_ctx *c, uint32_t round, float al
   g.alpha = alpha;
   g.next_sent = c->counters.p + 0;
   g.pairs = c->counters.p + 1;
+  g.fm_window = make_fastmod((uint32_t)c->o.window);
+  g.fm_vocab1 = make_fastmod((uint32_t)(c->vocab_size - 1));
   const int blocks = c->o.deterministic ? 1 : c->sm_count * 8;
   const int threads = c->o.deterministic ? 32 : 256;
   CK(cudaEventRecord(c->ev0, c->stream), "train_round");
@@ -927,12 +939,26 @@ extern "C" felog_status felog_train_round(felog_ctx *c, uint32_t round, float al
       case 128: k_sgns_cbow<128><<<blocks, threads, 0, c->stream>>>(g); break;
       case 256: k_sgns_cbow<256><<<blocks, threads, 0, c->stream>>>(g); break;
     }
+  } else if (c->o.negative == 5) {
+    switch (c->o.size) {
+      case 32: k_sgns_skipgram<32, 5><<<blocks, threads, 0, c->stream>>>(g); break;
+      case 64: k_sgns_skipgram<64, 5><<<blocks, threads, 0, c->stream>>>(g); break;
+      case 128: k_sgns_skipgram<128, 5><<<blocks, threads, 0, c->stream>>>(g); break;
+      case 256: k_sgns_skipgram<256, 5><<<blocks, threads, 0, c->stream>>>(g); break;
+    }
+  } else if (c->o.negative == 7) {
+    switch (c->o.size) {
+      case 32: k_sgns_skipgram<32, 7><<<blocks, threads, 0, c->stream>>>(g); break;
+      case 64: k_sgns_skipgram<64, 7><<<blocks, threads, 0, c->stream>>>(g); break;
+      case 128: k_sgns_skipgram<128, 7><<<blocks, threads, 0, c->stream>>>(g); break;
+      case 256: k_sgns_skipgram<256, 7><<<blocks, threads, 0, c->stream>>>(g); break;
+    }
   } else {
     switch (c->o.size) {
-      case 32: k_sgns_skipgram<32><<<blocks, threads, 0, c->stream>>>(g); break;
-      case 64: k_sgns_skipgram<64><<<blocks, threads, 0, c->stream>>>(g); break;
-      case 128: k_sgns_skipgram<128><<<blocks, threads, 0, c->stream>>>(g); break;
-      case 256: k_sgns_skipgram<256><<<blocks, threads, 0, c->stream>>>(g); break;
+      case 32: k_sgns_skipgram_any<32><<<blocks, threads, 0, c->stream>>>(g); break;
+      case 64: k_sgns_skipgram_any<64><<<blocks, threads, 0, c->stream>>>(g); break;
+      case 128: k_sgns_skipgram_any<128><<<blocks, threads, 0, c->stream>>>(g); break;
+      case 256: k_sgns_skipgram_any<256><<<blocks, threads, 0, c->stream>>>(g); break;
     }
   }
   c->launches++;

@@ -17,6 +17,29 @@ namespace felog {
 
 constexpr int kMaxNeg = 15;
 constexpr int kChunk = 8;  // targets whose rows are loaded together
+constexpr unsigned long long kUnigramSlots = 100000000ULL;  // table_size, word2vec.cu:171
+
+// x % d for a 64-bit x and a fixed 32-bit d, by a precomputed reciprocal
+// m = floor(2^64 / d): q = mulhi(x, m) is floor(x / d) or one less, so one
+// correction step gives the exact remainder.
+struct FastMod {
+  unsigned long long m;
+  uint32_t d;
+};
+
+inline FastMod make_fastmod(uint32_t d) {
+  FastMod f;
+  f.d = d;
+  f.m = d <= 1 ? 0ULL : (unsigned long long)(((unsigned __int128)1 << 64) / d);
+  return f;
+}
+
+__device__ __forceinline__ uint32_t fastmod(unsigned long long x, const FastMod &f) {
+  if (f.d <= 1) return 0;
+  unsigned long long q = __umul64hi(x, f.m);
+  unsigned long long r = x - q * (unsigned long long)f.d;
+  return (uint32_t)(r >= f.d ? r - f.d : r);
+}
 
 struct SgArgs {
   float *syn0;
@@ -35,6 +58,8 @@ struct SgArgs {
   float alpha;
   unsigned long long *next_sent;
   unsigned long long *pairs;
+  FastMod fm_window;  // % window
+  FastMod fm_vocab1;  // % (vocab_size - 1)
 };
 
 template <int J>
@@ -113,9 +138,10 @@ __device__ __forceinline__ float sg_grad(float f, int label, const float *s_exp,
   return __fmul_rn(__fsub_rn((float)label, s_exp[idx]), alpha);
 }
 
-// skip_gram_kernel semantics (word2vec.cu:442-536, hs = 0) per warp.
+// skip_gram_kernel semantics (word2vec.cu:442-536, hs = 0) per warp, any
+// number of negatives (chunks of kChunk targets).
 template <int DIM>
-__global__ void __launch_bounds__(256) k_sgns_skipgram(SgArgs a) {
+__global__ void __launch_bounds__(256) k_sgns_skipgram_any(SgArgs a) {
   constexpr int J = DIM / 32;
   __shared__ float s_exp[1000];
   for (int i = threadIdx.x; i < 1000; i += blockDim.x) s_exp[i] = a.exp_table[i];
@@ -193,6 +219,119 @@ __global__ void __launch_bounds__(256) k_sgns_skipgram(SgArgs a) {
         }
         red_row<J>(xrow, neu);
       }
+    }
+  }
+  if (lane == 0 && my_pairs) atomicAdd(a.pairs, my_pairs);
+}
+
+// skip_gram_kernel semantics for a fixed number of negatives NK, pipelined:
+// the draw sequence of the reference's LCG does not depend on the rows, so
+// the next (center, context) pair and its K unigram-table slots are produced
+// while the current pair is trained, and the table loads of the next pair are
+// in flight during the current pair's row loads and updates.  The LCG steps
+// happen in the reference's order: one window draw per center
+// (word2vec.cu:458-459), then K negative draws per context in range
+// (:502-505).
+template <int DIM, int NK>
+__global__ void __launch_bounds__(256) k_sgns_skipgram(SgArgs a) {
+  constexpr int J = DIM / 32;
+  constexpr int NT = NK + 1;
+  __shared__ float s_exp[1000];
+  for (int i = threadIdx.x; i < 1000; i += blockDim.x) s_exp[i] = a.exp_table[i];
+  __syncthreads();
+  const int lane = lane_id();
+  unsigned long long my_pairs = 0;
+  for (;;) {
+    unsigned long long s = 0;
+    if (lane == 0) s = atomicAdd(a.next_sent, 1ULL);
+    s = __shfl_sync(0xffffffffu, s, 0);
+    if (s >= a.n_sent) break;
+    const long long sb = (long long)a.sent_start[s], se = (long long)a.sent_start[s + 1];
+    unsigned long long nr = a.blk[s];
+    long long pos = sb - 1;
+    int aa = 0, hi = 0, word = 0;
+    // next valid pair: center word, context row, K table slots and fallbacks
+    auto advance = [&](int &w_out, int &l1_out, int32_t (&tv)[NK], int (&fb)[NK]) -> bool {
+      for (;;) {
+        if (aa >= hi) {
+          pos++;
+          if (pos >= se) return false;
+          word = __ldg(&a.sen[pos]);
+          nr = nr * 2514903917ULL + 11ULL;
+          const int b = (int)fastmod(nr, a.fm_window);
+          aa = b;
+          hi = a.window * 2 + 1 - b;
+        }
+        const int ca = aa++;
+        if (ca == a.window) continue;
+        const long long c = pos - a.window + ca;
+        if (c < sb || c >= se) continue;
+        w_out = word;
+        l1_out = __ldg(&a.sen[c]);
+#pragma unroll
+        for (int q = 0; q < NK; q++) {
+          nr = nr * 25214903917ULL + 11ULL;
+          tv[q] = __ldg(&a.table[(nr >> 16) % kUnigramSlots]);
+          fb[q] = (int)fastmod(nr, a.fm_vocab1) + 1;
+        }
+        return true;
+      }
+    };
+    int c_word = 0, c_l1 = 0;
+    int32_t c_tv[NK];
+    int c_fb[NK];
+    bool have = advance(c_word, c_l1, c_tv, c_fb);
+    while (have) {
+      int n_word = 0, n_l1 = 0;
+      int32_t n_tv[NK];
+      int n_fb[NK];
+      const bool nhave = advance(n_word, n_l1, n_tv, n_fb);
+      // targets of the current pair (word2vec.cu:496-507)
+      int tg[NT];
+      tg[0] = c_word;
+#pragma unroll
+      for (int q = 0; q < NK; q++) {
+        const int t = c_tv[q] == 0 ? c_fb[q] : c_tv[q];
+        tg[q + 1] = t == c_word ? -1 : t;
+      }
+      float *xrow = a.syn0 + (long long)c_l1 * DIM;
+      float x[J];
+      ld_row<J>(xrow, x);
+      float y[NT][J];
+#pragma unroll
+      for (int q = 0; q < NT; q++)
+        if (tg[q] >= 0) ld_row<J>(a.syn1 + (long long)tg[q] * DIM, y[q]);
+      float neu[J];
+#pragma unroll
+      for (int j = 0; j < J; j++) neu[j] = 0.0f;
+#pragma unroll
+      for (int q = 0; q < NT; q++) {
+        if (tg[q] < 0) continue;
+        const float f = sg_dot<J>(x, y[q]);
+        const float g = sg_grad(f, q == 0 ? 1 : 0, s_exp, a.alpha);
+        float upd[J];
+#pragma unroll
+        for (int j = 0; j < J; j++) {
+          neu[j] = __fmaf_rn(g, y[q][j], neu[j]);
+          upd[j] = __fmul_rn(g, x[j]);
+        }
+        red_row<J>(a.syn1 + (long long)tg[q] * DIM, upd);
+#pragma unroll
+        for (int r = q + 1; r < NT; r++)
+          if (tg[r] == tg[q])
+#pragma unroll
+            for (int j = 0; j < J; j++) y[r][j] = __fadd_rn(y[q][j], upd[j]);
+      }
+      red_row<J>(xrow, neu);
+      my_pairs++;
+      c_word = n_word;
+      c_l1 = n_l1;
+#pragma unroll
+      for (int q = 0; q < NK; q++) {
+        c_tv[q] = n_tv[q];
+        c_fb[q] = n_fb[q];
+      }
+      have = nhave;
     }
   }
   if (lane == 0 && my_pairs) atomicAdd(a.pairs, my_pairs);

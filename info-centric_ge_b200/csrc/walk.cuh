@@ -53,6 +53,7 @@ struct WalkArgs {
   uint64_t *sent_ptr;            // per sentence: token offset in arena
   uint32_t *sent_len;
   unsigned int *visit_freq;      // cumulative visits per vertex (KL)
+  const double *corr_tab;        // t(S, fi) table (k_corr_table), or NULL
   unsigned int *next_walker;
   unsigned long long *stats;     // [tokens, traces, iterations, long]
   int *err;
@@ -66,19 +67,39 @@ __device__ __forceinline__ void corr_init(Corr &c) {
   c.H = 0.0; c.EH = 0.0; c.ES = 1.0; c.EHS = 0.0; c.EHH = 0.0; c.ESS = 1.0; c.R = 1.0; c.S = 1.0;
 }
 
-// Correlation::iterate with step_k = 1 (walk.hpp:309-366).
-__device__ __forceinline__ void corr_iterate(Corr &c, double fi) {
-  const double Sn = c.S;
+// The entropy increment t(S, fi) of Correlation::iterateHn with step_k = 1
+// (walk.hpp:296-316): log2 of SnSn_div_Snp1Snp1(S) times, for a revisit,
+// FjFj_div_FiFi(fi).  It depends only on the integers S and fi.
+__device__ __forceinline__ double corr_t(double Sn, double fi) {
   const double Snp1 = __dadd_rn(Sn, 1.0);
   double ss = __dmul_rn(pow(__ddiv_rn(Sn, Snp1), Sn), pow(__ddiv_rn(1.0, Snp1), 1.0));
-  double t;
-  if (fi == 0.0) {
-    t = log2(ss);
-  } else {
-    double fj = __dadd_rn(fi, 1.0);
-    double ff = __dmul_rn(pow(__ddiv_rn(fj, fi), fi), pow(fj, 1.0));
-    t = log2(__dmul_rn(ss, ff));
+  if (fi == 0.0) return log2(ss);
+  double fj = __dadd_rn(fi, 1.0);
+  double ff = __dmul_rn(pow(__ddiv_rn(fj, fi), fi), pow(fj, 1.0));
+  return log2(__dmul_rn(ss, ff));
+}
+
+// t(S, fi) for 1 <= S <= kCorrTableS and 0 <= fi <= S, computed once by
+// k_corr_table with corr_t itself, so a table entry is bit-identical to the
+// value the walker would compute; larger S falls back to corr_t.
+constexpr int kCorrTableS = 127;
+__device__ __forceinline__ uint32_t corr_tab_index(uint32_t S, uint32_t fi) { return S * (kCorrTableS + 1) + fi; }
+
+__global__ void k_corr_table(double *tab) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < (kCorrTableS + 1) * (kCorrTableS + 1);
+       i += gridDim.x * blockDim.x) {
+    uint32_t S = i / (kCorrTableS + 1), fi = i % (kCorrTableS + 1);
+    tab[i] = (S >= 1 && fi <= S) ? corr_t((double)S, (double)fi) : 0.0;
   }
+}
+
+// Correlation::iterate with step_k = 1 (walk.hpp:309-366).
+__device__ __forceinline__ void corr_iterate(Corr &c, uint32_t fi_u, const double *__restrict__ tab) {
+  const double Sn = c.S;
+  const double Snp1 = __dadd_rn(Sn, 1.0);
+  const double fi = (double)fi_u;
+  const uint32_t S_u = (uint32_t)Sn;
+  const double t = (tab && S_u <= (uint32_t)kCorrTableS) ? __ldg(&tab[corr_tab_index(S_u, fi_u)]) : corr_t(Sn, fi);
   const double H1 = __ddiv_rn(__dsub_rn(__dmul_rn(Sn, c.H), t), Snp1);
   const double Np1 = Snp1;  // N + 1 with N == S
   const double EH = __dadd_rn(c.EH, __ddiv_rn(__dsub_rn(H1, c.EH), Np1));
@@ -136,7 +157,7 @@ __device__ __forceinline__ bool path_push(const WalkArgs &a, PathBuf &pb, uint32
   return true;
 }
 
-__global__ void __launch_bounds__(256) k_walk(WalkArgs a) {
+__global__ void __launch_bounds__(256, 3) k_walk(WalkArgs a) {
   unsigned long long my_tok = 0, my_tr = 0, my_it = 0, my_long = 0;
   for (;;) {
     uint32_t k = atomicAdd(a.next_walker, 1u);
@@ -217,12 +238,12 @@ __global__ void __launch_bounds__(256) k_walk(WalkArgs a) {
       if (!path_push(a, pb, dst)) { ok = false; break; }
       bloom |= bloom_bit(dst);
       if (dst == cur) cnt_cur++;
-      corr_iterate(c, (double)fi);
+      corr_iterate(c, fi, a.corr_tab);
       if (corr_stop(c, step, a.min_len)) break;
       if (trace) {
         step++;
         if (!path_push(a, pb, cur)) { ok = false; break; }
-        corr_iterate(c, (double)cnt_cur);
+        corr_iterate(c, cnt_cur, a.corr_tab);
         cnt_cur++;
         if (corr_stop(c, step, a.min_len)) break;
       } else {
