@@ -51,7 +51,8 @@ TRAIN = dict(min_length=20, min_rounds=2, size=128, window=10, negative=5, sampl
              min_count=0)
 METRIC = "walk+SGNS corpus tokens/s (walk steps/s and SGNS words/s reported alongside)"
 WALK_BYTES_PER_STEP = 68      # 2 random 32-B sectors + 4-B token write
-SGNS_BYTES_PER_PAIR = 7168    # 14 rows x 128 x 4 B (read + write syn0 row and 6 syn1 rows)
+SGNS_BYTES_PER_PAIR = {"fp32": 7168,   # 14 rows x 128 x 4 B (read + write syn0 row and 6 syn1 rows)
+                       "bf16": 3584}   # the same rows at 2 B per value (FP32 master rows: top 1%)
 
 
 def log(*a):
@@ -216,7 +217,8 @@ def bench_mine(args):
     cfg = CONFIGS[args.config]
     g = make_graph(cfg)
     V = g["v_num"]
-    f = fb.Felog(v_num=V, device=local, seed=1000 + rank, **TRAIN)
+    prec = args.precision
+    f = fb.Felog(v_num=V, device=local, seed=1000 + rank, precision=1 if prec == "bf16" else 0, **TRAIN)
     f.load_graph(g["edges"], V)
     f.init_model()
     min_r = TRAIN["min_rounds"]
@@ -262,7 +264,7 @@ def bench_mine(args):
     e2e_value = sum_over_ranks(pg, e2e["tokens"]) / (e2e_ms * 1e-3)
     peak, peak_kind = measured_peaks()
     # dominant kernel: the skip-gram pass
-    sg_achieved = cnt["pairs"] * SGNS_BYTES_PER_PAIR / (cnt["train_ms"] * 1e-3) / 1e9
+    sg_achieved = cnt["pairs"] * SGNS_BYTES_PER_PAIR[prec] / (cnt["train_ms"] * 1e-3) / 1e9
     walk_achieved = cnt["tokens"] * WALK_BYTES_PER_STEP / (cnt["walk_ms"] * 1e-3) / 1e9
     out = {
         "metric": METRIC,
@@ -275,18 +277,21 @@ def bench_mine(args):
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f32 tables, f64 walk statistics",
+        "dtype": ("f32 tables" if prec == "fp32" else "bf16 tables (f32 master rows for the top 1%), f32 arithmetic")
+                 + ", f64 walk statistics",
         "data": "synthetic (seeded R-MAT, see config)",
-        "config": {"workload": cfg["workload"], "v_num": V, "train_edges": int(len(g["edges"])),
+        "config": {"workload": cfg["workload"] if prec == "fp32" else cfg["workload"].replace("plain FP32", "BF16 form"),
+                   "v_num": V, "train_edges": int(len(g["edges"])),
                    "dim": 128, "window": 10, "negative": 5, "sample": 1e-3, "min_L": 20, "min_R": 2,
-                   "skip_gram": True, "reuse_neg": 0, "l2": "inputs larger than L2 (CSR + tables > 126 MB)",
+                   "skip_gram": True, "reuse_neg": 0, "precision": prec,
+                   "l2": "inputs larger than L2 (CSR + tables > 126 MB)",
                    "parallelism": f"replicas x{world}"},
         "walk_steps_per_s": cnt["tokens"] / (cnt["walk_ms"] * 1e-3),
         "sgns_words_per_s": cnt["words"] / ((cnt["train_ms"] + cnt["plan_ms"]) * 1e-3),
         "phase_ms_per_step": {k: cnt[k] / args.steps for k in ("walk_ms", "plan_ms", "train_ms", "budget_ms")},
         "tokens_per_step": cnt["tokens"] / args.steps,
         "pairs_per_step": cnt["pairs"] / args.steps,
-        "roofline": {"kernel": "k_sgns_skipgram<128>", "bound": "hbm", "achieved": sg_achieved, "peak": peak,
+        "roofline": {"kernel": f"k_sgns_skipgram<128, 5, Rows{prec.upper()}>", "bound": "hbm", "achieved": sg_achieved, "peak": peak,
                      "unit": "GB/s", "frac": sg_achieved / peak, "traffic": None,
                      "peak_source": peak_kind,
                      "walk_kernel": {"achieved": walk_achieved, "frac": walk_achieved / peak,
@@ -358,6 +363,7 @@ def main():
     ap.add_argument("--config", default="c2", choices=sorted(CONFIGS))
     ap.add_argument("--ref-walkers", type=int, default=200000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "bf16"])
     args = ap.parse_args()
     if args.impl == "reference":
         bench_reference(args)

@@ -98,6 +98,7 @@ typedef struct felog_opts {
   uint64_t seed;            /* Philox key for walks, neighbour choice, rounding */
   uint64_t long_arena_tokens; /* spill arena for long walks (0: automatic) */
   uint64_t wait_limit;      /* spin limit of device-side waits (0: default) */
+  int64_t hot_rows;         /* BF16 mode: FP32 master rows (0: the top 1% of the vocabulary, at least 1) */
 } felog_opts;
 
 typedef struct felog_ctx felog_ctx;
@@ -223,6 +224,15 @@ felog_status felog_train_round(felog_ctx *ctx, uint32_t round, float alpha, felo
 /* rows in vocabulary order, logical dimension order, FP32 */
 felog_status felog_get_embeddings(felog_ctx *ctx, float *syn0, float *syn1, uint64_t cap_floats);
 felog_status felog_set_embeddings(felog_ctx *ctx, const float *syn0, const float *syn1);
+/* No counterpart in the reference (precision study).  For n (context row,
+ * target row, label) triples in vocabulary-row indices: dots[i] = the FP32
+ * dot of syn0[ctx] and syn1[target] formed exactly as the trainer forms it
+ * from the stored rows (FP32 or BF16 storage), and batch_loss[b] = the FP64
+ * sum over triples i with batch_of[i] == b of -log sigma(label ? f : -f).
+ * Host buffers. */
+felog_status felog_score_pairs(felog_ctx *ctx, const int32_t *ctx_rows, const int32_t *tgt_rows,
+                               const int8_t *labels, const uint64_t *batch_of, uint64_t n, uint64_t n_batches,
+                               float *dots, double *batch_loss);
 /* the batch plan of the last felog_train_round (parity checks) */
 felog_status felog_plan_size(felog_ctx *ctx, uint64_t *n_sentences, uint64_t *n_sen, uint64_t *n_batches);
 felog_status felog_get_plan(felog_ctx *ctx, int32_t *sen, uint64_t *sent_start, uint64_t *batch_first,

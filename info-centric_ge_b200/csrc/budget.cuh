@@ -15,11 +15,12 @@
 #pragma once
 
 #include "common.cuh"
+#include "sgns.cuh"
 
 namespace felog {
 
 struct ConvArgs {
-  const float *syn0;  // interleaved rows
+  SgArgs rows;  // syn0 rows (FP32 and, in BF16 mode, BF16 parts), interleaved
   const uint32_t *id2offset;
   const uint64_t *row_ptr;
   const uint2 *adj;
@@ -70,14 +71,7 @@ __device__ __forceinline__ float tree_sum(float (&p)[J]) {
   return r;
 }
 
-template <int J>
-__device__ __forceinline__ void ld_row_plain(const float *row, float (&r)[J]) {
-  const float *p = row + lane_id() * J;
-#pragma unroll
-  for (int j = 0; j < J; j++) r[j] = p[j];
-}
-
-template <int DIM>
+template <int DIM, class P>
 __global__ void __launch_bounds__(256) k_converge(ConvArgs a) {
   constexpr int J = DIM / 32;
   __shared__ uint32_t s_choice[8][30];
@@ -98,7 +92,7 @@ __global__ void __launch_bounds__(256) k_converge(ConvArgs a) {
       __syncwarp();
     }
     float x[J];
-    ld_row_plain<J>(a.syn0 + (uint64_t)a.id2offset[v] * DIM, x);
+    row_load<DIM, P>(a.rows, 0, a.id2offset[v], x);
     float px[J];
 #pragma unroll
     for (int j = 0; j < J; j++) px[j] = __fmul_rn(x[j], x[j]);
@@ -111,7 +105,7 @@ __global__ void __launch_bounds__(256) k_converge(ConvArgs a) {
       if (a.id2offset[u] == 0xFFFFFFFFu) continue;  // neighbour without a row
       used++;
       float y[J];
-      ld_row_plain<J>(a.syn0 + (uint64_t)a.id2offset[u] * DIM, y);
+      row_load<DIM, P>(a.rows, 0, a.id2offset[u], y);
       float pd[J], py[J];
 #pragma unroll
       for (int j = 0; j < J; j++) {

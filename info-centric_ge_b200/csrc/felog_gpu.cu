@@ -107,7 +107,9 @@ struct felog_ctx {
   bool use_thr = false;
   DevBuf<int32_t> table;
   DevBuf<float> exp_table;
-  DevBuf<float> syn0, syn1;
+  DevBuf<float> syn0, syn1;        // FP32 rows 0..n_f32-1 (all rows in FP32 mode)
+  DevBuf<uint16_t> syn0_bf, syn1_bf;  // BF16 mode: rows n_f32.. as BF16 bits
+  long long n_f32 = 0;
   bool model_ready = false;
   DevBuf<LcgJump> jump;
 
@@ -265,7 +267,7 @@ extern "C" void felog_destroy(felog_ctx *c) {
   c->visit_freq.release(); c->counters.release(); c->derr.release(); c->inj_idx_off.release();
   c->inj_p_off.release(); c->inj_idx.release(); c->inj_p.release(); c->flags_tmp.release();
   c->kl_partial.release(); c->corr_tab.release(); c->id2offset.release(); c->thr.release(); c->table.release();
-  c->exp_table.release(); c->syn0.release(); c->syn1.release(); c->jump.release();
+  c->exp_table.release(); c->syn0.release(); c->syn1.release(); c->syn0_bf.release(); c->syn1_bf.release(); c->jump.release();
   c->p_cand.release(); c->p_draws.release(); c->p_cons.release(); c->p_kept.release(); c->p_blk.release();
   c->p_state.release(); c->p_neg_state.release(); c->p_out_off.release(); c->p_batch_first.release();
   c->p_sen.release(); c->p_negs.release(); c->sim.release(); c->cub_tmp.release(); c->out_tmp.release();
@@ -688,17 +690,33 @@ extern "C" felog_status felog_get_visit_freq(felog_ctx *c, uint64_t *freq) {
 
 namespace {
 
-__global__ void k_init_syn0(float *syn0, uint64_t vocab_size, int dim, const LcgJump *J) {
+// FP32 -> BF16 bits, round to nearest even (finite inputs)
+__host__ __device__ inline uint32_t bf16_rne(float v) {
+#ifdef __CUDA_ARCH__
+  const uint32_t b = __float_as_uint(v);
+#else
+  uint32_t b;
+  memcpy(&b, &v, 4);
+#endif
+  return (b + 0x7FFFu + ((b >> 16) & 1u)) >> 16;
+}
+
+// InitNet rows (word2vec.cu:893-896) in the interleaved layout; in BF16 mode
+// rows n_f32.. are stored rounded to nearest.
+__global__ void k_init_syn0(float *syn0, uint16_t *syn0_bf, uint64_t n_f32, uint64_t vocab_size, int dim,
+                            const LcgJump *J) {
   const uint64_t n = vocab_size * (uint64_t)dim;
   const int Jn = dim / 32;
   for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < n; e += (uint64_t)gridDim.x * blockDim.x) {
-    // element e of the row-major LCG fill (word2vec.cu:893-896): state after e + 1 steps from 1
+    // element e of the row-major LCG fill: state after e + 1 steps from 1
     unsigned long long s = lcg_jump(*J, 1ULL, e + 1);
     float q = __fdiv_rn((float)(s & 0xFFFF), 65536.0f);
     float v = (float)__ddiv_rn(__dsub_rn((double)q, 0.5), (double)dim);
     uint64_t row = e / dim;
     int logical = (int)(e % dim);
-    syn0[row * dim + (uint64_t)(logical % 32) * Jn + logical / 32] = v;
+    const uint64_t col = (uint64_t)(logical % 32) * Jn + logical / 32;
+    if (row < n_f32) syn0[row * dim + col] = v;
+    else syn0_bf[(row - n_f32) * dim + col] = (uint16_t)bf16_rne(v);
   }
 }
 
@@ -713,7 +731,8 @@ extern "C" felog_status felog_init_model(felog_ctx *c) {
   if (c->o.negative < 1 || c->o.negative > kMaxNeg)
     return fail(c, FELOG_INVALID_ARG, "-negative %d: supported range is 1..%d", c->o.negative, kMaxNeg);
   if (c->o.window < 1) return fail(c, FELOG_INVALID_ARG, "-window must be >= 1");
-  if (c->o.precision != FELOG_FP32) return fail(c, FELOG_INVALID_ARG, "precision mode not available");
+  if (c->o.precision != FELOG_FP32 && c->o.precision != FELOG_BF16)
+    return fail(c, FELOG_INVALID_ARG, "precision %d: use FELOG_FP32 or FELOG_BF16", c->o.precision);
   CK(cudaSetDevice(c->device), "init_model");
   // vocabulary from degrees: stable sort, degree descending (word2vec.cu:834-862, :734-755)
   const uint32_t V = c->V;
@@ -783,11 +802,22 @@ extern "C" felog_status felog_init_model(felog_ctx *c) {
   if (c->use_thr) CK(cudaMemcpy(c->thr.p, thr.data(), 2 * thr.size(), cudaMemcpyHostToDevice), "init_model");
   CK(c->exp_table.ensure(1000), "init_model");
   CK(cudaMemcpy(c->exp_table.p, et, sizeof et, cudaMemcpyHostToDevice), "init_model");
+  // BF16 mode: FP32 master rows for the top 1% of the vocabulary (at least one row)
+  c->n_f32 = size;
+  if (c->o.precision == FELOG_BF16)
+    c->n_f32 = std::min<long long>(size, c->o.hot_rows > 0 ? c->o.hot_rows : std::max<long long>(1, (size + 99) / 100));
   const uint64_t nel = (uint64_t)size * dim;
-  CK(c->syn0.ensure(nel), "init_model: syn0");
-  CK(c->syn1.ensure(nel), "init_model: syn1");
-  CK(cudaMemsetAsync(c->syn1.p, 0, 4 * nel, c->stream), "init_model");
-  k_init_syn0<<<grid_for(c, nel, 256), 256, 0, c->stream>>>(c->syn0.p, (uint64_t)size, dim, c->jump.p);
+  const uint64_t nf = (uint64_t)c->n_f32 * dim, nb = nel - nf;
+  CK(c->syn0.ensure(nf), "init_model: syn0");
+  CK(c->syn1.ensure(nf), "init_model: syn1");
+  CK(cudaMemsetAsync(c->syn1.p, 0, 4 * nf, c->stream), "init_model");
+  if (nb) {
+    CK(c->syn0_bf.ensure(nb), "init_model: syn0 (BF16)");
+    CK(c->syn1_bf.ensure(nb), "init_model: syn1 (BF16)");
+    CK(cudaMemsetAsync(c->syn1_bf.p, 0, 2 * nb, c->stream), "init_model");
+  }
+  k_init_syn0<<<grid_for(c, nel, 256), 256, 0, c->stream>>>(c->syn0.p, c->syn0_bf.p, (uint64_t)c->n_f32,
+                                                             (uint64_t)size, dim, c->jump.p);
   c->launches++;
   CK(cudaGetLastError(), "init_model");
   CK(c->sim.ensure(V), "init_model");
@@ -895,6 +925,24 @@ felog_status plan_round(felog_ctx *c, float *ms) {
   return FELOG_OK;
 }
 
+template <int D, class P>
+void launch_dim(felog_ctx *c, const SgArgs &g, int blocks, int threads) {
+  if (c->o.cbow) k_sgns_cbow<D, P><<<blocks, threads, 0, c->stream>>>(g);
+  else if (c->o.negative == 5) k_sgns_skipgram<D, 5, P><<<blocks, threads, 0, c->stream>>>(g);
+  else if (c->o.negative == 7) k_sgns_skipgram<D, 7, P><<<blocks, threads, 0, c->stream>>>(g);
+  else k_sgns_skipgram_any<D, P><<<blocks, threads, 0, c->stream>>>(g);
+}
+
+template <class P>
+void launch_trainer(felog_ctx *c, const SgArgs &g, int blocks, int threads) {
+  switch (c->o.size) {
+    case 32: launch_dim<32, P>(c, g, blocks, threads); break;
+    case 64: launch_dim<64, P>(c, g, blocks, threads); break;
+    case 128: launch_dim<128, P>(c, g, blocks, threads); break;
+    case 256: launch_dim<256, P>(c, g, blocks, threads); break;
+  }
+}
+
 }  // namespace
 
 extern "C" felog_status felog_train_round(felog_ctx *c, uint32_t round, float alpha, felog_train_stats *stats) {
@@ -929,38 +977,25 @@ extern "C" felog_status felog_train_round(felog_ctx *c, uint32_t round, float al
   g.pairs = c->counters.p + 1;
   g.fm_window = make_fastmod((uint32_t)c->o.window);
   g.fm_vocab1 = make_fastmod((uint32_t)(c->vocab_size - 1));
+  g.syn0_bf = c->syn0_bf.p;
+  g.syn1_bf = c->syn1_bf.p;
+  g.n_hot = c->n_f32;
+  g.sr_seed = sr_hash((uint32_t)c->o.seed ^ sr_hash((uint32_t)(c->o.seed >> 32) + round * 0x9E3779B9u));
+  {
+    // negative-draw LCG x -> 25214903917 x + 11 (word2vec.cu:502) composed q + 1 times
+    unsigned long long A = 1, C = 0;
+    for (int q = 0; q < kMaxNeg; q++) {
+      A = A * 25214903917ULL;
+      C = C * 25214903917ULL + 11ULL;
+      g.lcg_a[q] = A;
+      g.lcg_c[q] = C;
+    }
+  }
   const int blocks = c->o.deterministic ? 1 : c->sm_count * 8;
   const int threads = c->o.deterministic ? 32 : 256;
   CK(cudaEventRecord(c->ev0, c->stream), "train_round");
-  if (c->o.cbow) {
-    switch (c->o.size) {
-      case 32: k_sgns_cbow<32><<<blocks, threads, 0, c->stream>>>(g); break;
-      case 64: k_sgns_cbow<64><<<blocks, threads, 0, c->stream>>>(g); break;
-      case 128: k_sgns_cbow<128><<<blocks, threads, 0, c->stream>>>(g); break;
-      case 256: k_sgns_cbow<256><<<blocks, threads, 0, c->stream>>>(g); break;
-    }
-  } else if (c->o.negative == 5) {
-    switch (c->o.size) {
-      case 32: k_sgns_skipgram<32, 5><<<blocks, threads, 0, c->stream>>>(g); break;
-      case 64: k_sgns_skipgram<64, 5><<<blocks, threads, 0, c->stream>>>(g); break;
-      case 128: k_sgns_skipgram<128, 5><<<blocks, threads, 0, c->stream>>>(g); break;
-      case 256: k_sgns_skipgram<256, 5><<<blocks, threads, 0, c->stream>>>(g); break;
-    }
-  } else if (c->o.negative == 7) {
-    switch (c->o.size) {
-      case 32: k_sgns_skipgram<32, 7><<<blocks, threads, 0, c->stream>>>(g); break;
-      case 64: k_sgns_skipgram<64, 7><<<blocks, threads, 0, c->stream>>>(g); break;
-      case 128: k_sgns_skipgram<128, 7><<<blocks, threads, 0, c->stream>>>(g); break;
-      case 256: k_sgns_skipgram<256, 7><<<blocks, threads, 0, c->stream>>>(g); break;
-    }
-  } else {
-    switch (c->o.size) {
-      case 32: k_sgns_skipgram_any<32><<<blocks, threads, 0, c->stream>>>(g); break;
-      case 64: k_sgns_skipgram_any<64><<<blocks, threads, 0, c->stream>>>(g); break;
-      case 128: k_sgns_skipgram_any<128><<<blocks, threads, 0, c->stream>>>(g); break;
-      case 256: k_sgns_skipgram_any<256><<<blocks, threads, 0, c->stream>>>(g); break;
-    }
-  }
+  if (c->o.precision == FELOG_BF16) launch_trainer<RowsBF16>(c, g, blocks, threads);
+  else launch_trainer<RowsF32>(c, g, blocks, threads);
   c->launches++;
   CK(cudaGetLastError(), "train_round: launch");
   CK(cudaEventRecord(c->ev1, c->stream), "train_round");
@@ -1013,14 +1048,16 @@ extern "C" felog_status felog_get_plan(felog_ctx *c, int32_t *sen, uint64_t *sen
 
 namespace {
 
-// interleaved rows -> logical order (see sgns.cuh)
-__global__ void k_unpermute(const float *src, float *dst, uint64_t rows, int dim) {
+// interleaved rows -> logical order (see sgns.cuh); rows n_f32.. from BF16
+__global__ void k_unpermute(const float *src, const uint16_t *src_bf, uint64_t n_f32, float *dst, uint64_t rows,
+                            int dim) {
   const int Jn = dim / 32;
   const uint64_t n = rows * (uint64_t)dim;
   for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < n; e += (uint64_t)gridDim.x * blockDim.x) {
     uint64_t r = e / dim;
     int l = (int)(e % dim);
-    dst[e] = src[r * dim + (uint64_t)(l % 32) * Jn + l / 32];
+    const uint64_t col = (uint64_t)(l % 32) * Jn + l / 32;
+    dst[e] = r < n_f32 ? src[r * dim + col] : __uint_as_float((uint32_t)src_bf[(r - n_f32) * dim + col] << 16);
   }
 }
 
@@ -1037,7 +1074,9 @@ extern "C" felog_status felog_get_embeddings(felog_ctx *c, float *syn0, float *s
   for (int which = 0; which < 2; which++) {
     float *dst = which ? syn1 : syn0;
     if (!dst) continue;
-    k_unpermute<<<grid_for(c, nel, 256), 256, 0, c->stream>>>(which ? c->syn1.p : c->syn0.p, c->out_tmp.p,
+    k_unpermute<<<grid_for(c, nel, 256), 256, 0, c->stream>>>(which ? c->syn1.p : c->syn0.p,
+                                                               which ? c->syn1_bf.p : c->syn0_bf.p,
+                                                               (uint64_t)c->n_f32, c->out_tmp.p,
                                                                (uint64_t)c->vocab_size, dim);
     c->launches++;
     CK(cudaGetLastError(), "get_embeddings");
@@ -1066,15 +1105,92 @@ extern "C" felog_status felog_set_embeddings(felog_ctx *c, const float *syn0, co
   if (!c) return FELOG_INVALID_ARG;
   if (!c->model_ready) return fail(c, FELOG_NOT_READY, "model not initialised");
   const int dim = c->o.size;
-  const uint64_t nel = (uint64_t)c->vocab_size * dim;
-  std::vector<float> buf(nel);
+  const uint64_t nf = (uint64_t)c->n_f32 * dim, nel = (uint64_t)c->vocab_size * dim;
+  std::vector<float> buf(nf);
+  std::vector<uint16_t> bbuf(nel - nf);
   for (int which = 0; which < 2; which++) {
     const float *src = which ? syn1 : syn0;
     if (!src) continue;
     for (uint64_t r = 0; r < (uint64_t)c->vocab_size; r++)
-      for (int l = 0; l < dim; l++) buf[r * dim + phys_index(dim, l)] = src[r * dim + l];
-    CK(cudaMemcpy(which ? c->syn1.p : c->syn0.p, buf.data(), 4 * nel, cudaMemcpyHostToDevice), "set_embeddings");
+      for (int l = 0; l < dim; l++) {
+        const float v = src[r * dim + l];
+        if (r < (uint64_t)c->n_f32) buf[r * dim + phys_index(dim, l)] = v;
+        else bbuf[(r - c->n_f32) * dim + phys_index(dim, l)] = (uint16_t)bf16_rne(v);  // BF16 rows: nearest
+      }
+    CK(cudaMemcpy(which ? c->syn1.p : c->syn0.p, buf.data(), 4 * nf, cudaMemcpyHostToDevice), "set_embeddings");
+    if (nel > nf)
+      CK(cudaMemcpy(which ? c->syn1_bf.p : c->syn0_bf.p, bbuf.data(), 2 * (nel - nf), cudaMemcpyHostToDevice),
+         "set_embeddings");
   }
+  return FELOG_OK;
+}
+
+extern "C" felog_status felog_score_pairs(felog_ctx *c, const int32_t *ctx_rows, const int32_t *tgt_rows,
+                                          const int8_t *labels, const uint64_t *batch_of, uint64_t n,
+                                          uint64_t n_batches, float *dots, double *batch_loss) {
+  if (!c || (n && (!ctx_rows || !tgt_rows || !labels || !batch_of || !dots)) || (n_batches && !batch_loss))
+    return FELOG_INVALID_ARG;
+  if (!c->model_ready) return fail(c, FELOG_NOT_READY, "model not initialised");
+  for (uint64_t i = 0; i < n; i++) {
+    if (ctx_rows[i] < 0 || ctx_rows[i] >= c->vocab_size || tgt_rows[i] < 0 || tgt_rows[i] >= c->vocab_size)
+      return fail(c, FELOG_INVALID_ARG, "score_pairs: row index out of range at %llu", (unsigned long long)i);
+    if (batch_of[i] >= n_batches) return fail(c, FELOG_INVALID_ARG, "score_pairs: batch index out of range");
+  }
+  if (!n) {
+    for (uint64_t b = 0; b < n_batches; b++) batch_loss[b] = 0.0;
+    return FELOG_OK;
+  }
+  CK(cudaSetDevice(c->device), "score_pairs");
+  int32_t *d_ctx = nullptr, *d_tgt = nullptr;
+  int8_t *d_lab = nullptr;
+  uint64_t *d_b = nullptr;
+  float *d_dots = nullptr;
+  double *d_loss = nullptr;
+  cudaError_t e = cudaMalloc(&d_ctx, 4 * n);
+  if (e == cudaSuccess) e = cudaMalloc(&d_tgt, 4 * n);
+  if (e == cudaSuccess) e = cudaMalloc(&d_lab, n);
+  if (e == cudaSuccess) e = cudaMalloc(&d_b, 8 * n);
+  if (e == cudaSuccess) e = cudaMalloc(&d_dots, 4 * n);
+  if (e == cudaSuccess) e = cudaMalloc(&d_loss, 8 * std::max<uint64_t>(n_batches, 1));
+  if (e == cudaSuccess) e = cudaMemcpy(d_ctx, ctx_rows, 4 * n, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(d_tgt, tgt_rows, 4 * n, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(d_lab, labels, n, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(d_b, batch_of, 8 * n, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemset(d_loss, 0, 8 * std::max<uint64_t>(n_batches, 1));
+  if (e == cudaSuccess) {
+    SgArgs g{};
+    g.syn0 = c->syn0.p;
+    g.syn1 = c->syn1.p;
+    g.syn0_bf = c->syn0_bf.p;
+    g.syn1_bf = c->syn1_bf.p;
+    g.n_hot = c->n_f32;
+    const int blocks = grid_for(c, n * 32, 256);
+    const bool bf = c->o.precision == FELOG_BF16;
+    switch (c->o.size) {
+#define FELOG_SP(D)                                                                                     \
+  case D:                                                                                               \
+    if (bf) k_score_pairs<D, RowsBF16><<<blocks, 256, 0, c->stream>>>(g, d_ctx, d_tgt, d_lab, d_b, n, d_dots, d_loss); \
+    else k_score_pairs<D, RowsF32><<<blocks, 256, 0, c->stream>>>(g, d_ctx, d_tgt, d_lab, d_b, n, d_dots, d_loss);    \
+    break;
+      FELOG_SP(32)
+      FELOG_SP(64)
+      FELOG_SP(128)
+      FELOG_SP(256)
+#undef FELOG_SP
+    }
+    c->launches++;
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e == cudaSuccess) e = cudaMemcpy(dots, d_dots, 4 * n, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && n_batches) e = cudaMemcpy(batch_loss, d_loss, 8 * n_batches, cudaMemcpyDeviceToHost);
+  }
+  cudaFree(d_ctx);
+  cudaFree(d_tgt);
+  cudaFree(d_lab);
+  cudaFree(d_b);
+  cudaFree(d_dots);
+  cudaFree(d_loss);
+  if (e != cudaSuccess) return cuda_fail(c, e, "score_pairs");
   return FELOG_OK;
 }
 
@@ -1086,7 +1202,9 @@ extern "C" felog_status felog_budget_check(felog_ctx *c, uint32_t round, felog_b
   CK(cudaSetDevice(c->device), "budget_check");
   CK(cudaMemsetAsync(c->counters.p, 0, sizeof(unsigned long long) * 4, c->stream), "budget_check");
   ConvArgs a{};
-  a.syn0 = c->syn0.p;
+  a.rows.syn0 = c->syn0.p;
+  a.rows.syn0_bf = c->syn0_bf.p;
+  a.rows.n_hot = c->n_f32;
   a.id2offset = c->id2offset.p;
   a.row_ptr = c->row_ptr.p;
   a.adj = c->adj.p;
@@ -1098,11 +1216,18 @@ extern "C" felog_status felog_budget_check(felog_ctx *c, uint32_t round, felog_b
   a.counters = c->counters.p;
   CK(cudaEventRecord(c->ev0, c->stream), "budget_check");
   const int blocks = grid_for(c, (uint64_t)c->V * 32, 256, 8);
+  const bool bf = c->o.precision == FELOG_BF16;
   switch (c->o.size) {
-    case 32: k_converge<32><<<blocks, 256, 0, c->stream>>>(a); break;
-    case 64: k_converge<64><<<blocks, 256, 0, c->stream>>>(a); break;
-    case 128: k_converge<128><<<blocks, 256, 0, c->stream>>>(a); break;
-    case 256: k_converge<256><<<blocks, 256, 0, c->stream>>>(a); break;
+#define FELOG_CV(D)                                                            \
+  case D:                                                                      \
+    if (bf) k_converge<D, RowsBF16><<<blocks, 256, 0, c->stream>>>(a);         \
+    else k_converge<D, RowsF32><<<blocks, 256, 0, c->stream>>>(a);             \
+    break;
+    FELOG_CV(32)
+    FELOG_CV(64)
+    FELOG_CV(128)
+    FELOG_CV(256)
+#undef FELOG_CV
   }
   c->launches++;
   k_count_stopped<<<grid_for(c, c->V, 256), 256, 0, c->stream>>>(c->stop.p, c->V, c->counters.p + 2);

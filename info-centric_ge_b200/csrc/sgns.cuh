@@ -1,7 +1,7 @@
-// Skip-gram negative-sampling kernels.
+// Skip-gram / CBOW negative-sampling kernels.
 //
 // One warp per sentence (Hogwild across warps, like the reference's one block
-// per sentence).  Row layout is interleaved: for a row of DIM = 32 * J floats,
+// per sentence).  Row layout is interleaved: for a row of DIM = 32 * J values,
 // physical position lane * J + j holds logical dimension lane + 32 j, so each
 // lane moves its J values with one vector load / one vector reduction and the
 // dot product below sums the products in exactly the order of the reference's
@@ -9,7 +9,20 @@
 // then halve).  Every multiply-add that the reference kernel fuses is written
 // as an explicit fmaf and every other operation as a rounded intrinsic, so a
 // single warp reproduces the reference's sequential semantics bit for bit.
+//
+// Row storage policies (template parameter P):
+//   RowsF32  - every row FP32; updates are vector reductions (the reference's
+//              atomicAdd, word2vec.cu:530, :533).
+//   RowsBF16 - the n_hot most frequent vocabulary rows (rows 0..n_hot-1: the
+//              vocabulary is sorted by degree) are FP32 master rows updated by
+//              reductions; every other row is stored in BF16, computed on in
+//              FP32 and written back as the stochastically rounded new value
+//              with a plain store (Hogwild).  The rounding bits come from a
+//              hash of (seed, sentence, pair, slot, lane), not from the
+//              schedule, so one warp is still deterministic.
 #pragma once
+
+#include <cstring>
 
 #include "common.cuh"
 
@@ -42,8 +55,12 @@ __device__ __forceinline__ uint32_t fastmod(unsigned long long x, const FastMod 
 }
 
 struct SgArgs {
-  float *syn0;
+  float *syn0;  // FP32 rows: all rows, or the n_hot master rows (RowsBF16)
   float *syn1;
+  uint16_t *syn0_bf;  // RowsBF16: rows n_hot.. as BF16 bits, row r at (r - n_hot) * DIM
+  uint16_t *syn1_bf;
+  long long n_hot;
+  uint32_t sr_seed;
   const int32_t *sen;
   const uint64_t *sent_start;  // n_sent + 1
   const uint32_t *blk;         // index of the sentence in its batch
@@ -60,18 +77,20 @@ struct SgArgs {
   unsigned long long *pairs;
   FastMod fm_window;  // % window
   FastMod fm_vocab1;  // % (vocab_size - 1)
+  // the negative-draw LCG advanced by q + 1 steps: x -> lcg_a[q] x + lcg_c[q]
+  unsigned long long lcg_a[kMaxNeg];
+  unsigned long long lcg_c[kMaxNeg];
 };
 
+// ------------------------------------------------------------ row access
 template <int J>
-__device__ __forceinline__ void ld_row(const float *row, float (&r)[J]) {
-  const float *p = row + lane_id() * J;
-  if constexpr (J == 8) {
-    float4 u = __ldcg(reinterpret_cast<const float4 *>(p));
-    float4 v = __ldcg(reinterpret_cast<const float4 *>(p) + 1);
-    r[0] = u.x; r[1] = u.y; r[2] = u.z; r[3] = u.w; r[4] = v.x; r[5] = v.y; r[6] = v.z; r[7] = v.w;
-  } else if constexpr (J == 4) {
-    float4 u = __ldcg(reinterpret_cast<const float4 *>(p));
-    r[0] = u.x; r[1] = u.y; r[2] = u.z; r[3] = u.w;
+__device__ __forceinline__ void ld_f32(const float *p, float (&r)[J]) {
+  if constexpr (J % 4 == 0) {
+#pragma unroll
+    for (int k = 0; k < J / 4; k++) {
+      float4 u = __ldcg(reinterpret_cast<const float4 *>(p) + k);
+      r[4 * k] = u.x; r[4 * k + 1] = u.y; r[4 * k + 2] = u.z; r[4 * k + 3] = u.w;
+    }
   } else if constexpr (J == 2) {
     float2 u = __ldcg(reinterpret_cast<const float2 *>(p));
     r[0] = u.x; r[1] = u.y;
@@ -90,18 +109,132 @@ __device__ __forceinline__ void red_add_v2(float *p, float a, float b) {
 }
 
 template <int J>
-__device__ __forceinline__ void red_row(float *row, const float (&u)[J]) {
-  float *p = row + lane_id() * J;
-  if constexpr (J == 8) {
-    red_add_v4(p, u[0], u[1], u[2], u[3]);
-    red_add_v4(p + 4, u[4], u[5], u[6], u[7]);
-  } else if constexpr (J == 4) {
-    red_add_v4(p, u[0], u[1], u[2], u[3]);
+__device__ __forceinline__ void red_f32(float *p, const float (&u)[J]) {
+  if constexpr (J % 4 == 0) {
+#pragma unroll
+    for (int k = 0; k < J / 4; k++) red_add_v4(p + 4 * k, u[4 * k], u[4 * k + 1], u[4 * k + 2], u[4 * k + 3]);
   } else if constexpr (J == 2) {
     red_add_v2(p, u[0], u[1]);
   } else {
     atomicAdd(p, u[0]);
   }
+}
+
+// 32-bit integer mixer (multiply / xor-shift), the source of the rounding bits
+__host__ __device__ __forceinline__ uint32_t sr_hash(uint32_t x) {
+  x ^= x >> 16;
+  x *= 0x7FEB352Du;
+  x ^= x >> 15;
+  x *= 0x846CA68Bu;
+  x ^= x >> 16;
+  return x;
+}
+
+// Rounding streams.  One hash per (sentence, pair, lane) gives the lane's key;
+// the stream of row slot `slot` (target index d = 0..K for syn1 rows,
+// kSlotCtx (+ window position for CBOW) for syn0 rows) starts at
+// key + slot * 0x27D4EB2F and takes one LCG step per two values: the word
+// R = x ^ (x >> 16) of the new state x gives its low 16 bits to the lane's
+// value 2k and its high 16 bits to value 2k + 1.  Every value's 16 bits are
+// uniform, so each rounding is unbiased; the streams depend on (seed,
+// sentence, pair, slot, lane) only.
+constexpr uint32_t kSlotCtx = 256;
+__host__ __device__ __forceinline__ uint32_t lane_key(uint32_t seed, uint64_t s, uint32_t pair, uint32_t lane) {
+  return sr_hash(seed ^ ((uint32_t)s * 0x9E3779B1u + pair * 0x85EBCA77u + lane * 0xC2B2AE3Du));
+}
+__host__ __device__ __forceinline__ uint32_t slot_stream(uint32_t key, uint32_t slot) {
+  return key + slot * 0x27D4EB2Fu;
+}
+__device__ __forceinline__ uint32_t sr_word(uint32_t &st) {
+  st = st * 1664525u + 1013904223u;
+  return st ^ (st >> 16);
+}
+// Two FP32 values to packed BF16 by stochastic rounding in one instruction
+// (sm_100a cvt.rs): hi goes to the upper half with random bits r >> 16, lo to
+// the lower half with r & 0xFFFF; each is (FP32 bits + 16 random bits) >> 16,
+// i.e. the magnitude rounds up with probability equal to the dropped
+// fraction.  (.satfinite only matters beyond the BF16 range.)
+__device__ __forceinline__ uint32_t sr_bf16x2(float hi, float lo, uint32_t r) {
+  uint32_t d;
+  asm("cvt.rs.satfinite.bf16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(hi), "f"(lo), "r"(r));
+  return d;
+}
+__device__ __forceinline__ float bf16_lo(uint32_t w) { return __uint_as_float(w << 16); }
+__device__ __forceinline__ float bf16_hi(uint32_t w) { return __uint_as_float(w & 0xFFFF0000u); }
+
+struct RowsF32 {
+  static constexpr bool kBF16 = false;
+};
+struct RowsBF16 {
+  static constexpr bool kBF16 = true;
+};
+
+// load row `row` of table `which` (0: syn0, 1: syn1) into the lane's J values
+template <int DIM, class P>
+__device__ __forceinline__ void row_load(const SgArgs &a, int which, long long row, float (&r)[DIM / 32]) {
+  constexpr int J = DIM / 32;
+  const int lane = lane_id();
+  if constexpr (P::kBF16) {
+    if (row >= a.n_hot) {
+      const uint16_t *b = (which ? a.syn1_bf : a.syn0_bf) + (row - a.n_hot) * DIM + lane * J;
+      if constexpr (J == 8) {
+        uint4 u = __ldcg(reinterpret_cast<const uint4 *>(b));
+        const uint32_t w[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+          r[2 * k] = bf16_lo(w[k]);
+          r[2 * k + 1] = bf16_hi(w[k]);
+        }
+      } else if constexpr (J == 4) {
+        uint2 u = __ldcg(reinterpret_cast<const uint2 *>(b));
+        r[0] = bf16_lo(u.x); r[1] = bf16_hi(u.x); r[2] = bf16_lo(u.y); r[3] = bf16_hi(u.y);
+      } else if constexpr (J == 2) {
+        uint32_t u = __ldcg(reinterpret_cast<const unsigned int *>(b));
+        r[0] = bf16_lo(u); r[1] = bf16_hi(u);
+      } else {
+        r[0] = __uint_as_float((uint32_t)__ldcg(reinterpret_cast<const unsigned short *>(b)) << 16);
+      }
+      return;
+    }
+  }
+  ld_f32<J>((which ? a.syn1 : a.syn0) + row * DIM + lane * J, r);
+}
+
+// Add u to row `row` whose value, as this warp read it, is cur.  FP32 rows:
+// vector reduction, cur unchanged, returns false.  BF16 rows: cur becomes the
+// stored value SR(cur + u) (plain store), returns true.
+template <int DIM, class P>
+__device__ __forceinline__ bool row_update(const SgArgs &a, int which, long long row, const float (&u)[DIM / 32],
+                                           float (&cur)[DIM / 32], uint32_t stream) {
+  constexpr int J = DIM / 32;
+  const int lane = lane_id();
+  if constexpr (P::kBF16) {
+    if (row >= a.n_hot) {
+      constexpr int W = (J + 1) / 2;
+      uint32_t w[W];
+#pragma unroll
+      for (int k = 0; k < W; k++) {
+        const float lo = __fadd_rn(cur[2 * k], u[2 * k]);
+        const float hi = 2 * k + 1 < J ? __fadd_rn(cur[2 * k + 1], u[2 * k + 1]) : 0.0f;
+        w[k] = sr_bf16x2(hi, lo, sr_word(stream));
+        cur[2 * k] = bf16_lo(w[k]);
+        if (2 * k + 1 < J) cur[2 * k + 1] = bf16_hi(w[k]);
+      }
+      uint16_t *b = (which ? a.syn1_bf : a.syn0_bf) + (row - a.n_hot) * DIM + lane * J;
+      if constexpr (J == 8) {
+        *reinterpret_cast<uint4 *>(b) = make_uint4(w[0], w[1], w[2], w[3]);
+      } else if constexpr (J == 4) {
+        *reinterpret_cast<uint2 *>(b) = make_uint2(w[0], w[1]);
+      } else if constexpr (J == 2) {
+        *reinterpret_cast<unsigned int *>(b) = w[0];
+      } else {
+        *reinterpret_cast<unsigned short *>(b) = (unsigned short)w[0];
+      }
+      return true;
+    }
+  }
+  red_f32<J>((which ? a.syn1 : a.syn0) + row * DIM + lane * J, u);
+  return false;
 }
 
 // dot product in the reference tree order (FSIZE = DIM / 2)
@@ -129,6 +262,60 @@ __device__ __forceinline__ float sg_dot(const float (&x)[J], const float (&y)[J]
   }
 }
 
+// Dot products of x against up to 8 rows y[0..NT) at once, each bit-identical
+// to sg_dot.  Every lane first folds its J products per target as sg_dot does;
+// then a transposing butterfly: at xor distance 16 a lane keeps the partial
+// sums of half of the targets and hands the other half to its partner, at 8 a
+// quarter, at 4 an eighth, then plain xor 2 and 1.  Each partial is the sum
+// of the same two halves as in sg_dot (IEEE addition commutes), so the values
+// are identical, for 7 shuffles instead of 5 per target.  Lane l ends with
+// the dot of target butterfly_target(l).
+__device__ __forceinline__ int butterfly_target(int lane) {
+  return ((lane >> 4) & 1) * 4 + ((lane >> 3) & 1) * 2 + ((lane >> 2) & 1);
+}
+__device__ __forceinline__ int butterfly_lane(int target) {
+  return ((target >> 2) & 1) * 16 + ((target >> 1) & 1) * 8 + (target & 1) * 4;
+}
+
+template <int J, int NT>
+__device__ __forceinline__ float multi_dot(const float (&x)[J], const float (&y)[NT][J]) {
+  static_assert(NT <= 8 && J >= 2, "up to 8 targets, at least two values per lane");
+  const int lane = lane_id();
+  float v[8];
+#pragma unroll
+  for (int q = 0; q < 8; q++) {
+    if (q < NT) {
+      float s[J / 2];
+#pragma unroll
+      for (int j = 0; j < J / 2; j++) s[j] = __fmaf_rn(x[j + J / 2], y[q][j + J / 2], __fmul_rn(x[j], y[q][j]));
+#pragma unroll
+      for (int h = J / 4; h >= 1; h >>= 1)
+#pragma unroll
+        for (int j = 0; j < h; j++) s[j] = __fadd_rn(s[j], s[j + h]);
+      v[q] = s[0];
+    } else {
+      v[q] = 0.0f;
+    }
+  }
+  const bool b4 = lane & 16, b3 = lane & 8, b2 = lane & 4;
+  float w[4];
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    const float keep = b4 ? v[k + 4] : v[k], send = b4 ? v[k] : v[k + 4];
+    w[k] = __fadd_rn(keep, __shfl_xor_sync(0xffffffffu, send, 16));
+  }
+  float u[2];
+#pragma unroll
+  for (int k = 0; k < 2; k++) {
+    const float keep = b3 ? w[k + 2] : w[k], send = b3 ? w[k] : w[k + 2];
+    u[k] = __fadd_rn(keep, __shfl_xor_sync(0xffffffffu, send, 8));
+  }
+  float z = __fadd_rn(b2 ? u[1] : u[0], __shfl_xor_sync(0xffffffffu, b2 ? u[0] : u[1], 4));
+  z = __fadd_rn(z, __shfl_xor_sync(0xffffffffu, z, 2));
+  z = __fadd_rn(z, __shfl_xor_sync(0xffffffffu, z, 1));
+  return z;
+}
+
 // g = (label - sigma(f)) * alpha with the reference's quantized sigmoid
 // (word2vec.cu:519-526; index (f + 6) * 83, EXP_TABLE_SIZE / MAX_EXP / 2 = 83).
 __device__ __forceinline__ float sg_grad(float f, int label, const float *s_exp, float alpha) {
@@ -138,23 +325,31 @@ __device__ __forceinline__ float sg_grad(float f, int label, const float *s_exp,
   return __fmul_rn(__fsub_rn((float)label, s_exp[idx]), alpha);
 }
 
+__device__ __forceinline__ void load_exp(const SgArgs &a, float *s_exp) {
+  for (int i = threadIdx.x; i < 1000; i += blockDim.x) s_exp[i] = a.exp_table[i];
+  __syncthreads();
+}
+
+__device__ __forceinline__ bool claim_sentence(const SgArgs &a, unsigned long long &s) {
+  unsigned long long v = 0;
+  if (lane_id() == 0) v = atomicAdd(a.next_sent, 1ULL);
+  s = __shfl_sync(0xffffffffu, v, 0);
+  return s < a.n_sent;
+}
+
 // skip_gram_kernel semantics (word2vec.cu:442-536, hs = 0) per warp, any
 // number of negatives (chunks of kChunk targets).
-template <int DIM>
+template <int DIM, class P>
 __global__ void __launch_bounds__(256) k_sgns_skipgram_any(SgArgs a) {
   constexpr int J = DIM / 32;
   __shared__ float s_exp[1000];
-  for (int i = threadIdx.x; i < 1000; i += blockDim.x) s_exp[i] = a.exp_table[i];
-  __syncthreads();
-  const int lane = lane_id();
+  load_exp(a, s_exp);
   unsigned long long my_pairs = 0;
-  for (;;) {
-    unsigned long long s = 0;
-    if (lane == 0) s = atomicAdd(a.next_sent, 1ULL);
-    s = __shfl_sync(0xffffffffu, s, 0);
-    if (s >= a.n_sent) break;
+  unsigned long long s;
+  while (claim_sentence(a, s)) {
     const long long sb = (long long)a.sent_start[s], se = (long long)a.sent_start[s + 1];
     unsigned long long nr = a.blk[s];
+    uint32_t pair = 0;
     for (long long pos = sb; pos < se; pos++) {
       const int word = a.sen[pos];
       nr = nr * 2514903917ULL + 11ULL;  // the reference's window LCG (word2vec.cu:458)
@@ -164,13 +359,14 @@ __global__ void __launch_bounds__(256) k_sgns_skipgram_any(SgArgs a) {
         const long long c = pos - a.window + aa;
         if (c < sb || c >= se) continue;
         const int l1 = a.sen[c];
-        float *xrow = a.syn0 + (long long)l1 * DIM;
+        const uint32_t key = P::kBF16 ? lane_key(a.sr_seed, s, pair, lane_id()) : 0u;
         float x[J];
-        ld_row<J>(xrow, x);
+        row_load<DIM, P>(a, 0, l1, x);
         float neu[J];
 #pragma unroll
         for (int j = 0; j < J; j++) neu[j] = 0.0f;
         my_pairs++;
+        pair++;
         for (int d0 = 0; d0 <= a.negative; d0 += kChunk) {
           int tg[kChunk];
           int lab[kChunk];
@@ -196,7 +392,7 @@ __global__ void __launch_bounds__(256) k_sgns_skipgram_any(SgArgs a) {
           }
 #pragma unroll
           for (int q = 0; q < kChunk; q++)
-            if (tg[q] >= 0) ld_row<J>(a.syn1 + (long long)tg[q] * DIM, y[q]);
+            if (tg[q] >= 0) row_load<DIM, P>(a, 1, tg[q], y[q]);
 #pragma unroll
           for (int q = 0; q < kChunk; q++) {
             if (tg[q] < 0) continue;
@@ -208,50 +404,54 @@ __global__ void __launch_bounds__(256) k_sgns_skipgram_any(SgArgs a) {
               neu[j] = __fmaf_rn(g, y[q][j], neu[j]);
               upd[j] = __fmul_rn(g, x[j]);
             }
-            red_row<J>(a.syn1 + (long long)tg[q] * DIM, upd);
+            const bool stored = row_update<DIM, P>(a, 1, tg[q], upd, y[q], slot_stream(key, d0 + q));
             // a later target with the same row sees this update
 #pragma unroll
             for (int r = q + 1; r < kChunk; r++)
               if (tg[r] == tg[q])
 #pragma unroll
-                for (int j = 0; j < J; j++) y[r][j] = __fadd_rn(y[q][j], upd[j]);
+                for (int j = 0; j < J; j++) y[r][j] = stored ? y[q][j] : __fadd_rn(y[q][j], upd[j]);
           }
         }
-        red_row<J>(xrow, neu);
+        row_update<DIM, P>(a, 0, l1, neu, x, slot_stream(key, kSlotCtx));
       }
     }
   }
-  if (lane == 0 && my_pairs) atomicAdd(a.pairs, my_pairs);
+  if (lane_id() == 0 && my_pairs) atomicAdd(a.pairs, my_pairs);
 }
 
-// skip_gram_kernel semantics for a fixed number of negatives NK, pipelined:
-// the draw sequence of the reference's LCG does not depend on the rows, so
-// the next (center, context) pair and its K unigram-table slots are produced
-// while the current pair is trained, and the table loads of the next pair are
-// in flight during the current pair's row loads and updates.  The LCG steps
-// happen in the reference's order: one window draw per center
-// (word2vec.cu:458-459), then K negative draws per context in range
-// (:502-505).
-template <int DIM, int NK>
-__global__ void __launch_bounds__(256) k_sgns_skipgram(SgArgs a) {
+// skip_gram_kernel semantics for a fixed number of negatives NK, pipelined.
+// The draw sequence of the reference's LCG does not depend on the rows, so the
+// next (center, context) pair and its unigram-table slots are produced while
+// the current pair trains: the next pair's table loads are in flight during
+// the current pair's row loads and updates.  Lane q < NK computes negative q
+// directly: the LCG state after q + 1 steps is an affine map of the state
+// before the pair's draws (lcg_a, lcg_c), so the K draws of the reference's
+// loop (:502-505) cost one multiply-add per lane; the window draw (:458-459)
+// stays one step per center.  With distinct targets the K + 1 scores come
+// from one multi_dot and each lane evaluates one gradient; a pair whose
+// targets repeat a row takes the sequential path, where the later target sees
+// the earlier update as in the reference.
+template <int DIM, int NK, class P>
+__global__ void __launch_bounds__(256, DIM >= 256 ? 2 : 4) k_sgns_skipgram(SgArgs a) {
   constexpr int J = DIM / 32;
   constexpr int NT = NK + 1;
+  constexpr bool kMulti = J >= 2 && NT <= 8;
+  static_assert(NK < 32, "one lane per negative");
   __shared__ float s_exp[1000];
-  for (int i = threadIdx.x; i < 1000; i += blockDim.x) s_exp[i] = a.exp_table[i];
-  __syncthreads();
+  load_exp(a, s_exp);
   const int lane = lane_id();
+  const unsigned long long my_a = lane < NK ? a.lcg_a[lane] : 0ULL;
+  const unsigned long long my_c = lane < NK ? a.lcg_c[lane] : 0ULL;
   unsigned long long my_pairs = 0;
-  for (;;) {
-    unsigned long long s = 0;
-    if (lane == 0) s = atomicAdd(a.next_sent, 1ULL);
-    s = __shfl_sync(0xffffffffu, s, 0);
-    if (s >= a.n_sent) break;
+  unsigned long long s;
+  while (claim_sentence(a, s)) {
     const long long sb = (long long)a.sent_start[s], se = (long long)a.sent_start[s + 1];
     unsigned long long nr = a.blk[s];
     long long pos = sb - 1;
     int aa = 0, hi = 0, word = 0;
-    // next valid pair: center word, context row, K table slots and fallbacks
-    auto advance = [&](int &w_out, int &l1_out, int32_t (&tv)[NK], int (&fb)[NK]) -> bool {
+    // next valid pair: center word, context row, and this lane's negative
+    auto advance = [&](int &w_out, int &l1_out, int &t_lane) -> bool {
       for (;;) {
         if (aa >= hi) {
           pos++;
@@ -268,69 +468,93 @@ __global__ void __launch_bounds__(256) k_sgns_skipgram(SgArgs a) {
         if (c < sb || c >= se) continue;
         w_out = word;
         l1_out = __ldg(&a.sen[c]);
-#pragma unroll
-        for (int q = 0; q < NK; q++) {
-          nr = nr * 25214903917ULL + 11ULL;
-          tv[q] = __ldg(&a.table[(nr >> 16) % kUnigramSlots]);
-          fb[q] = (int)fastmod(nr, a.fm_vocab1) + 1;
+        unsigned long long sq = 0;
+        t_lane = 0;
+        if (lane < NK) {
+          sq = my_a * nr + my_c;
+          const int32_t tv = __ldg(&a.table[(sq >> 16) % kUnigramSlots]);
+          t_lane = tv == 0 ? (int)fastmod(sq, a.fm_vocab1) + 1 : tv;
         }
+        nr = __shfl_sync(0xffffffffu, sq, NK - 1);  // state after the K draws
         return true;
       }
     };
-    int c_word = 0, c_l1 = 0;
-    int32_t c_tv[NK];
-    int c_fb[NK];
-    bool have = advance(c_word, c_l1, c_tv, c_fb);
+    int c_word = 0, c_l1 = 0, c_t = 0;
+    uint32_t pair = 0;
+    bool have = advance(c_word, c_l1, c_t);
     while (have) {
-      int n_word = 0, n_l1 = 0;
-      int32_t n_tv[NK];
-      int n_fb[NK];
-      const bool nhave = advance(n_word, n_l1, n_tv, n_fb);
-      // targets of the current pair (word2vec.cu:496-507)
+      int n_word = 0, n_l1 = 0, n_t = 0;
+      const bool nhave = advance(n_word, n_l1, n_t);
+      // targets of the current pair (word2vec.cu:496-507); -1: negative equal to the word
       int tg[NT];
       tg[0] = c_word;
 #pragma unroll
       for (int q = 0; q < NK; q++) {
-        const int t = c_tv[q] == 0 ? c_fb[q] : c_tv[q];
+        const int t = __shfl_sync(0xffffffffu, c_t, q);
         tg[q + 1] = t == c_word ? -1 : t;
       }
-      float *xrow = a.syn0 + (long long)c_l1 * DIM;
+      bool dup = false;
+#pragma unroll
+      for (int q = 2; q < NT; q++)
+#pragma unroll
+        for (int r = 1; r < q; r++) dup |= tg[q] >= 0 && tg[q] == tg[r];
       float x[J];
-      ld_row<J>(xrow, x);
+      row_load<DIM, P>(a, 0, c_l1, x);
       float y[NT][J];
 #pragma unroll
       for (int q = 0; q < NT; q++)
-        if (tg[q] >= 0) ld_row<J>(a.syn1 + (long long)tg[q] * DIM, y[q]);
+        if (tg[q] >= 0) row_load<DIM, P>(a, 1, tg[q], y[q]);
       float neu[J];
 #pragma unroll
       for (int j = 0; j < J; j++) neu[j] = 0.0f;
+      const uint32_t key = P::kBF16 ? lane_key(a.sr_seed, s, pair, lane_id()) : 0u;
+      bool done = false;
+      if constexpr (kMulti) {
+        if (!dup) {
+          const float z = multi_dot<J, NT>(x, y);
+          const int tq = butterfly_target(lane);
+          const float gv = tq < NT ? sg_grad(z, tq == 0 ? 1 : 0, s_exp, a.alpha) : 0.0f;
 #pragma unroll
-      for (int q = 0; q < NT; q++) {
-        if (tg[q] < 0) continue;
-        const float f = sg_dot<J>(x, y[q]);
-        const float g = sg_grad(f, q == 0 ? 1 : 0, s_exp, a.alpha);
-        float upd[J];
+          for (int q = 0; q < NT; q++) {
+            const float g = __shfl_sync(0xffffffffu, gv, butterfly_lane(q));
+            if (tg[q] < 0) continue;
+            float upd[J];
 #pragma unroll
-        for (int j = 0; j < J; j++) {
-          neu[j] = __fmaf_rn(g, y[q][j], neu[j]);
-          upd[j] = __fmul_rn(g, x[j]);
+            for (int j = 0; j < J; j++) {
+              neu[j] = __fmaf_rn(g, y[q][j], neu[j]);
+              upd[j] = __fmul_rn(g, x[j]);
+            }
+            row_update<DIM, P>(a, 1, tg[q], upd, y[q], slot_stream(key, q));
+          }
+          done = true;
         }
-        red_row<J>(a.syn1 + (long long)tg[q] * DIM, upd);
-#pragma unroll
-        for (int r = q + 1; r < NT; r++)
-          if (tg[r] == tg[q])
-#pragma unroll
-            for (int j = 0; j < J; j++) y[r][j] = __fadd_rn(y[q][j], upd[j]);
       }
-      red_row<J>(xrow, neu);
+      if (!done) {
+#pragma unroll
+        for (int q = 0; q < NT; q++) {
+          if (tg[q] < 0) continue;
+          const float f = sg_dot<J>(x, y[q]);
+          const float g = sg_grad(f, q == 0 ? 1 : 0, s_exp, a.alpha);
+          float upd[J];
+#pragma unroll
+          for (int j = 0; j < J; j++) {
+            neu[j] = __fmaf_rn(g, y[q][j], neu[j]);
+            upd[j] = __fmul_rn(g, x[j]);
+          }
+          const bool stored = row_update<DIM, P>(a, 1, tg[q], upd, y[q], slot_stream(key, q));
+#pragma unroll
+          for (int r = q + 1; r < NT; r++)
+            if (tg[r] == tg[q])
+#pragma unroll
+              for (int j = 0; j < J; j++) y[r][j] = stored ? y[q][j] : __fadd_rn(y[q][j], upd[j]);
+        }
+      }
+      row_update<DIM, P>(a, 0, c_l1, neu, x, slot_stream(key, kSlotCtx));
       my_pairs++;
+      pair++;
       c_word = n_word;
       c_l1 = n_l1;
-#pragma unroll
-      for (int q = 0; q < NK; q++) {
-        c_tv[q] = n_tv[q];
-        c_fb[q] = n_fb[q];
-      }
+      c_t = n_t;
       have = nhave;
     }
   }
@@ -340,24 +564,21 @@ __global__ void __launch_bounds__(256) k_sgns_skipgram(SgArgs a) {
 // cbow_kernel semantics (word2vec.cu:538-646, hs = 0) per warp: the mean of
 // the window's context rows (summed in window order, then divided by the
 // count) is scored against the positive and K negatives; every context row
-// then receives the accumulated error.
-template <int DIM>
+// then receives the accumulated error.  Rounding streams (RowsBF16) are keyed
+// by the center's position in the sentence.
+template <int DIM, class P>
 __global__ void __launch_bounds__(256) k_sgns_cbow(SgArgs a) {
   constexpr int J = DIM / 32;
   __shared__ float s_exp[1000];
-  for (int i = threadIdx.x; i < 1000; i += blockDim.x) s_exp[i] = a.exp_table[i];
-  __syncthreads();
-  const int lane = lane_id();
+  load_exp(a, s_exp);
   unsigned long long my_pairs = 0;
-  for (;;) {
-    unsigned long long s = 0;
-    if (lane == 0) s = atomicAdd(a.next_sent, 1ULL);
-    s = __shfl_sync(0xffffffffu, s, 0);
-    if (s >= a.n_sent) break;
+  unsigned long long s;
+  while (claim_sentence(a, s)) {
     const long long sb = (long long)a.sent_start[s], se = (long long)a.sent_start[s + 1];
     unsigned long long nr = a.blk[s];
     for (long long pos = sb; pos < se; pos++) {
       const int word = a.sen[pos];
+      const uint32_t key = P::kBF16 ? lane_key(a.sr_seed, s, (uint32_t)(pos - sb), lane_id()) : 0u;
       nr = nr * 2514903917ULL + 11ULL;
       const int b = (int)(nr % (unsigned long long)a.window);
       float neu1[J], neu1e[J];
@@ -369,7 +590,7 @@ __global__ void __launch_bounds__(256) k_sgns_cbow(SgArgs a) {
         const long long c = pos - a.window + aa;
         if (c < sb || c >= se) continue;
         float x[J];
-        ld_row<J>(a.syn0 + (long long)a.sen[c] * DIM, x);
+        row_load<DIM, P>(a, 0, a.sen[c], x);
 #pragma unroll
         for (int j = 0; j < J; j++) neu1[j] = __fadd_rn(neu1[j], x[j]);
         cw++;
@@ -402,7 +623,7 @@ __global__ void __launch_bounds__(256) k_sgns_cbow(SgArgs a) {
         }
 #pragma unroll
         for (int q = 0; q < kChunk; q++)
-          if (tg[q] >= 0) ld_row<J>(a.syn1 + (long long)tg[q] * DIM, y[q]);
+          if (tg[q] >= 0) row_load<DIM, P>(a, 1, tg[q], y[q]);
 #pragma unroll
         for (int q = 0; q < kChunk; q++) {
           if (tg[q] < 0) continue;
@@ -414,23 +635,52 @@ __global__ void __launch_bounds__(256) k_sgns_cbow(SgArgs a) {
             neu1e[j] = __fmaf_rn(g, y[q][j], neu1e[j]);
             upd[j] = __fmul_rn(g, neu1[j]);
           }
-          red_row<J>(a.syn1 + (long long)tg[q] * DIM, upd);
+          const bool stored = row_update<DIM, P>(a, 1, tg[q], upd, y[q], slot_stream(key, d0 + q));
 #pragma unroll
           for (int r = q + 1; r < kChunk; r++)
             if (tg[r] == tg[q])
 #pragma unroll
-              for (int j = 0; j < J; j++) y[r][j] = __fadd_rn(y[q][j], upd[j]);
+              for (int j = 0; j < J; j++) y[r][j] = stored ? y[q][j] : __fadd_rn(y[q][j], upd[j]);
         }
       }
+      // every context row receives neu1e; a BF16 row is re-read so that a
+      // context that occurs twice in the window sees its first update
       for (int aa = b; aa < a.window * 2 + 1 - b; aa++) {
         if (aa == a.window) continue;
         const long long c = pos - a.window + aa;
         if (c < sb || c >= se) continue;
-        red_row<J>(a.syn0 + (long long)a.sen[c] * DIM, neu1e);
+        float x[J];
+        if constexpr (P::kBF16) row_load<DIM, P>(a, 0, a.sen[c], x);
+        row_update<DIM, P>(a, 0, a.sen[c], neu1e, x, slot_stream(key, kSlotCtx + aa));
       }
     }
   }
-  if (lane == 0 && my_pairs) atomicAdd(a.pairs, my_pairs);
+  if (lane_id() == 0 && my_pairs) atomicAdd(a.pairs, my_pairs);
+}
+
+// Scores of (context, target, label) triples for the precision study: the
+// dot of syn0[ctx] and syn1[target] exactly as the trainer forms it (FP32
+// products and tree from the stored rows) and each triple's negative-sampling
+// loss -log sigma(+-f) in FP64, summed per batch in FP64.
+template <int DIM, class P>
+__global__ void __launch_bounds__(256) k_score_pairs(SgArgs a, const int32_t *ctx, const int32_t *tgt,
+                                                     const int8_t *label, const uint64_t *batch_of, uint64_t n,
+                                                     float *dots, double *batch_loss) {
+  constexpr int J = DIM / 32;
+  const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nw = (gridDim.x * (uint64_t)blockDim.x) >> 5;
+  for (uint64_t i = warp; i < n; i += nw) {
+    float x[J], y[J];
+    row_load<DIM, P>(a, 0, ctx[i], x);
+    row_load<DIM, P>(a, 1, tgt[i], y);
+    const float f = sg_dot<J>(x, y);
+    if (lane_id() == 0) {
+      dots[i] = f;
+      const double z = label[i] ? (double)f : -(double)f;
+      const double l = z > 0 ? log1p(exp(-z)) : -z + log1p(exp(z));  // -log sigma(z)
+      atomicAdd(&batch_loss[batch_of[i]], l);
+    }
+  }
 }
 
 }  // namespace felog

@@ -43,6 +43,7 @@ class FelogOpts(ctypes.Structure):
         ("weighted", ctypes.c_int32), ("budget_mode", ctypes.c_int32), ("max_rounds", ctypes.c_int32),
         ("device", ctypes.c_int32), ("slot_len", ctypes.c_int32), ("seed", ctypes.c_uint64),
         ("long_arena_tokens", ctypes.c_uint64), ("wait_limit", ctypes.c_uint64),
+        ("hot_rows", ctypes.c_int64),
     ]
 
 
@@ -130,6 +131,7 @@ def gpu_lib():
         L.felog_get_embeddings.argtypes = [_P, _P, _P, ctypes.c_uint64]
         L.felog_set_embeddings.argtypes = [_P, _P, _P]
         L.felog_plan_size.argtypes = [_P, _P, _P, _P]
+        L.felog_score_pairs.argtypes = [_P, _P, _P, _P, _P, ctypes.c_uint64, ctypes.c_uint64, _P, _P]
         L.felog_get_plan.argtypes = [_P, _P, _P, _P, _P]
         L.felog_budget_check.argtypes = [_P, ctypes.c_uint32, ctypes.POINTER(BudgetStats)]
         L.felog_get_similarity.argtypes = [_P, _P]
@@ -328,6 +330,19 @@ class Felog:
         a = np.ascontiguousarray(syn0, np.float32) if syn0 is not None else None
         b = np.ascontiguousarray(syn1, np.float32) if syn1 is not None else None
         self._ck(self._L.felog_set_embeddings(self.h, _addr(a), _addr(b)))
+
+    def score_pairs(self, ctx_rows, tgt_rows, labels, batch_of, n_batches):
+        """FP32 dots of syn0[ctx] . syn1[tgt] as the trainer forms them, and the
+        FP64 negative-sampling loss summed per batch."""
+        c = np.ascontiguousarray(ctx_rows, np.int32)
+        t = np.ascontiguousarray(tgt_rows, np.int32)
+        lab = np.ascontiguousarray(labels, np.int8)
+        b = np.ascontiguousarray(batch_of, np.uint64)
+        dots = np.zeros(max(len(c), 1), np.float32)
+        loss = np.zeros(max(n_batches, 1), np.float64)
+        self._ck(self._L.felog_score_pairs(self.h, _addr(c), _addr(t), _addr(lab), _addr(b), len(c), n_batches,
+                                           _addr(dots), _addr(loss)))
+        return dots[: len(c)], loss[:n_batches]
 
     def plan(self):
         ns, nsen, nb = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()

@@ -554,6 +554,198 @@ void orc_cbow_batch(float *syn0, float *syn1, const float *exp_table, const int3
   }
 }
 
+/* ---- BF16 storage form (this project's precision form; no reference
+ * counterpart).  Rows 0..n_hot-1 are FP32 master rows updated by addition;
+ * rows n_hot.. are BF16 bit patterns, read as FP32 and written back as
+ * SR(value + update): 16 random bits added below the BF16 mantissa, then
+ * truncation.  The bits of one (pair, slot, lane) come from a keyed stream:
+ *   key    = H(seed ^ ((u32)s * 0x9E3779B1 + pair * 0x85EBCA77 + lane * 0xC2B2AE3D))
+ *   stream = key + slot * 0x27D4EB2F
+ *   word k = x ^ (x >> 16) with x = (stream = stream * 1664525 + 1013904223),
+ *            one per two values: its low 16 bits round the lane's value 2k,
+ *            its high 16 bits value 2k + 1
+ * (s: sentence index in the plan; pair: index of the (center, context) pair in
+ * the sentence, or of the center for CBOW)  * where H is a multiply / xor-shift mixer, slot = d (target index, 0 is the
+ * positive) for syn1 rows and 256 (+ window position a for CBOW) for syn0
+ * rows, and the lane's values j = 0, 1, 2, ... are the logical dimensions
+ * l, l + 32, l + 64, ... of lane l.  Everything else is skip_gram_kernel / cbow_kernel
+ * (word2vec.cu:442-646) exactly as in orc_skipgram_batch / orc_cbow_batch. */
+static uint32_t sr_h(uint32_t x) {
+  x ^= x >> 16;
+  x *= 0x7FEB352Du;
+  x ^= x >> 15;
+  x *= 0x846CA68Bu;
+  x ^= x >> 16;
+  return x;
+}
+uint32_t orc_lane_key(uint32_t seed, uint64_t s, uint32_t pair, uint32_t lane) {
+  return sr_h(seed ^ ((uint32_t)s * 0x9E3779B1u + pair * 0x85EBCA77u + lane * 0xC2B2AE3Du));
+}
+static float bf_to_f(uint16_t h) {
+  uint32_t b = (uint32_t)h << 16;
+  float f;
+  memcpy(&f, &b, 4);
+  return f;
+}
+static uint16_t f_to_bf_sr(float v, uint32_t r16) {
+  uint32_t b;
+  memcpy(&b, &v, 4);
+  return (uint16_t)((b + r16) >> 16);
+}
+typedef struct {
+  float *f32;
+  uint16_t *bf;
+  long long n_hot;
+  int dim;
+} mixed_rows;
+static void mr_get(const mixed_rows *m, long long row, float *out) {
+  if (row < m->n_hot) {
+    memcpy(out, m->f32 + row * m->dim, sizeof(float) * m->dim);
+  } else {
+    const uint16_t *b = m->bf + (row - m->n_hot) * m->dim;
+    for (int t = 0; t < m->dim; t++) out[t] = bf_to_f(b[t]);
+  }
+}
+/* row += u (FP32 rows) or row = SR(cur + u) (BF16 rows; cur = the row as read) */
+static void mr_add(const mixed_rows *m, long long row, const float *cur, const float *u, uint32_t seed, uint64_t s,
+                   uint32_t pair, uint32_t slot) {
+  if (row < m->n_hot) {
+    float *r = m->f32 + row * m->dim;
+    for (int t = 0; t < m->dim; t++) r[t] += u[t];
+    return;
+  }
+  uint16_t *b = m->bf + (row - m->n_hot) * m->dim;
+  for (int lane = 0; lane < 32; lane++) {
+    uint32_t st = orc_lane_key(seed, s, pair, (uint32_t)lane) + slot * 0x27D4EB2Fu, w = 0;
+    for (int j = 0; lane + 32 * j < m->dim; j++) {
+      int t = lane + 32 * j;
+      if ((j & 1) == 0) {
+        st = st * 1664525u + 1013904223u;
+        w = st ^ (st >> 16);
+      }
+      b[t] = f_to_bf_sr(cur[t] + u[t], (j & 1) ? (w >> 16) : (w & 0xFFFFu));
+    }
+  }
+}
+
+/* rounding seed of one training round, from the context seed */
+uint32_t orc_round_sr_seed(uint64_t seed, uint32_t round) {
+  return sr_h((uint32_t)seed ^ sr_h((uint32_t)(seed >> 32) + round * 0x9E3779B9u));
+}
+
+void orc_skipgram_bf16(float *syn0, uint16_t *syn0_bf, float *syn1, uint16_t *syn1_bf, long long n_hot,
+                       uint32_t sr_seed, const float *exp_table, const int32_t *table, int64_t table_size,
+                       long long vocab_size, const int32_t *sen, const uint64_t *sent_start,
+                       uint64_t first_sentence, uint64_t n_sentences, int window, int dim, int negative,
+                       float alpha) {
+  mixed_rows m0 = {syn0, syn0_bf, n_hot, dim}, m1 = {syn1, syn1_bf, n_hot, dim};
+  float x[512], y[512], neu1e[512], upd[512];
+  for (uint64_t blk = 0; blk < n_sentences; blk++) {
+    uint64_t s = first_sentence + blk;
+    long long ss = (long long)sent_start[s], se = (long long)sent_start[s + 1];
+    unsigned long next_random = (unsigned long)blk;
+    uint32_t pair = 0;
+    for (long long pos = ss; pos < se; pos++) {
+      int word = sen[pos];
+      if (word == -1) continue;
+      next_random = next_random * (unsigned long)2514903917 + 11;
+      int b = (int)(next_random % (unsigned long)window);
+      for (int a = b; a < window * 2 + 1 - b; a++) {
+        if (a == window) continue;
+        long long c = pos - window + a;
+        if (c < ss || c >= se) continue;
+        int last_word = sen[c];
+        if (last_word == -1) continue;
+        uint32_t pk = pair++;
+        mr_get(&m0, last_word, x);
+        for (int t = 0; t < dim; t++) neu1e[t] = 0;
+        for (int d = 0; d < negative + 1; d++) {
+          int target, label;
+          if (d == 0) {
+            target = word;
+            label = 1;
+          } else {
+            next_random = next_random * (unsigned long)25214903917 + 11;
+            target = table[(next_random >> 16) % (unsigned long)table_size];
+            if (target == 0) target = (int)(next_random % (unsigned long)(vocab_size - 1) + 1);
+            if (target == word) continue;
+            label = 0;
+          }
+          mr_get(&m1, target, y);
+          float f = sg_dot(x, y, dim);
+          float g = sg_gradient(f, label, exp_table, alpha);
+          for (int t = 0; t < dim; t++) {
+            neu1e[t] = fmaf(g, y[t], neu1e[t]);
+            upd[t] = g * x[t];
+          }
+          mr_add(&m1, target, y, upd, sr_seed, s, pk, (uint32_t)d);
+        }
+        mr_add(&m0, last_word, x, neu1e, sr_seed, s, pk, 256u);
+      }
+    }
+  }
+}
+
+void orc_cbow_bf16(float *syn0, uint16_t *syn0_bf, float *syn1, uint16_t *syn1_bf, long long n_hot,
+                   uint32_t sr_seed, const float *exp_table, const int32_t *table, int64_t table_size,
+                   long long vocab_size, const int32_t *sen, const uint64_t *sent_start, uint64_t first_sentence,
+                   uint64_t n_sentences, int window, int dim, int negative, float alpha) {
+  mixed_rows m0 = {syn0, syn0_bf, n_hot, dim}, m1 = {syn1, syn1_bf, n_hot, dim};
+  float x[512], y[512], neu1[512], neu1e[512], upd[512];
+  for (uint64_t blk = 0; blk < n_sentences; blk++) {
+    uint64_t s = first_sentence + blk;
+    long long ss = (long long)sent_start[s], se = (long long)sent_start[s + 1];
+    unsigned long next_random = (unsigned long)blk;
+    for (long long pos = ss; pos < se; pos++) {
+      int word = sen[pos];
+      if (word == -1) continue;
+      uint32_t pk = (uint32_t)(pos - ss);
+      for (int t = 0; t < dim; t++) neu1[t] = neu1e[t] = 0;
+      next_random = next_random * (unsigned long)2514903917 + 11;
+      int b = (int)(next_random % (unsigned long)window);
+      int cw = 0;
+      for (int a = b; a < window * 2 + 1 - b; a++) {
+        if (a == window) continue;
+        long long c = pos - window + a;
+        if (c < ss || c >= se || sen[c] == -1) continue;
+        mr_get(&m0, sen[c], x);
+        for (int t = 0; t < dim; t++) neu1[t] += x[t];
+        cw++;
+      }
+      if (!cw) continue;
+      for (int t = 0; t < dim; t++) neu1[t] /= cw;
+      for (int d = 0; d < negative + 1; d++) {
+        int target, label;
+        if (d == 0) {
+          target = word;
+          label = 1;
+        } else {
+          next_random = next_random * (unsigned long)25214903917 + 11;
+          target = table[(next_random >> 16) % (unsigned long)table_size];
+          if (target == 0) target = (int)(next_random % (unsigned long)(vocab_size - 1) + 1);
+          if (target == word) continue;
+          label = 0;
+        }
+        mr_get(&m1, target, y);
+        float f = sg_dot(neu1, y, dim);
+        float g = sg_gradient(f, label, exp_table, alpha);
+        for (int t = 0; t < dim; t++) {
+          neu1e[t] = fmaf(g, y[t], neu1e[t]);
+          upd[t] = g * neu1[t];
+        }
+        mr_add(&m1, target, y, upd, sr_seed, s, pk, (uint32_t)d);
+      }
+      for (int a = b; a < window * 2 + 1 - b; a++) {
+        if (a == window) continue;
+        long long c = pos - window + a;
+        if (c < ss || c >= se || sen[c] == -1) continue;
+        mr_get(&m0, sen[c], x);
+        mr_add(&m0, sen[c], x, neu1e, sr_seed, s, pk, 256u + (uint32_t)a);
+      }
+    }
+  }
+}
+
 void orc_init_net(float *syn0, float *syn1, long long vocab_size, int dim) {
   unsigned long long next_random = 1;
   for (long long a = 0; a < vocab_size; a++)

@@ -132,6 +132,21 @@ void orc_negreuse_batch(float *syn0, float *syn1, const float *exp_table, const 
                         const int32_t *negs, int window, int dim, int negative, float alpha);
 
 /* cbow_kernel, word2vec.cu:538-646 (negative sampling, hs = 0). */
+/* BF16 storage form of orc_skipgram_batch / orc_cbow_batch (FP32 master rows
+ * 0..n_hot-1, stochastically rounded BF16 rows after them; rule in
+ * felog_oracle.c).  syn*_bf hold (vocab_size - n_hot) * dim BF16 bit patterns,
+ * logical dimension order. */
+uint32_t orc_lane_key(uint32_t seed, uint64_t s, uint32_t pair, uint32_t lane);
+uint32_t orc_round_sr_seed(uint64_t seed, uint32_t round);
+void orc_skipgram_bf16(float *syn0, uint16_t *syn0_bf, float *syn1, uint16_t *syn1_bf, long long n_hot,
+                       uint32_t sr_seed, const float *exp_table, const int32_t *table, int64_t table_size,
+                       long long vocab_size, const int32_t *sen, const uint64_t *sent_start,
+                       uint64_t first_sentence, uint64_t n_sentences, int window, int dim, int negative,
+                       float alpha);
+void orc_cbow_bf16(float *syn0, uint16_t *syn0_bf, float *syn1, uint16_t *syn1_bf, long long n_hot,
+                   uint32_t sr_seed, const float *exp_table, const int32_t *table, int64_t table_size,
+                   long long vocab_size, const int32_t *sen, const uint64_t *sent_start, uint64_t first_sentence,
+                   uint64_t n_sentences, int window, int dim, int negative, float alpha);
 void orc_cbow_batch(float *syn0, float *syn1, const float *exp_table, const int32_t *table,
                     int64_t table_size, long long vocab_size, const int32_t *sen,
                     const uint64_t *sent_start, uint64_t first_sentence, uint64_t n_sentences,

@@ -82,6 +82,12 @@ def lib():
                                          i32p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float]
         L.orc_cbow_batch.argtypes = L.orc_skipgram_batch.argtypes
         L.orc_init_net.argtypes = [f32p, f32p, ctypes.c_longlong, ctypes.c_int]
+        L.orc_skipgram_bf16.argtypes = [f32p, u16p, f32p, u16p, ctypes.c_longlong, ctypes.c_uint32, f32p, i32p,
+                                        ctypes.c_int64, ctypes.c_longlong, i32p, u64p, ctypes.c_uint64,
+                                        ctypes.c_uint64, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float]
+        L.orc_cbow_bf16.argtypes = L.orc_skipgram_bf16.argtypes
+        L.orc_round_sr_seed.argtypes = [ctypes.c_uint64, ctypes.c_uint32]
+        L.orc_round_sr_seed.restype = ctypes.c_uint32
         L.orc_convergence.argtypes = [f32p, u32p, ctypes.c_int, ctypes.POINTER(Csr), u8p, ctypes.c_uint64,
                                       ctypes.c_uint32, f32p]
         L.orc_convergence.restype = ctypes.c_uint64
@@ -217,6 +223,42 @@ def skipgram_batch(syn0, syn1, exp_tab, table, vocab_size, sen, sent_start, firs
                    negative, alpha, cbow=False):
     fn = lib().orc_cbow_batch if cbow else lib().orc_skipgram_batch
     fn(ptr(syn0, f32p), ptr(syn1, f32p), ptr(exp_tab, f32p), ptr(table, i32p), len(table), vocab_size,
+       ptr(np.ascontiguousarray(sen, np.int32), i32p), ptr(np.ascontiguousarray(sent_start, np.uint64), u64p),
+       first, n, window, dim, negative, alpha)
+
+
+def bf16_rne(x):
+    """FP32 -> BF16 bit patterns, round to nearest even (finite values)."""
+    b = np.ascontiguousarray(x, np.float32).view(np.uint32).astype(np.uint64)
+    return ((b + 0x7FFF + ((b >> 16) & 1)) >> 16).astype(np.uint16)
+
+
+def bf16_to_f32(h):
+    return (np.asarray(h, np.uint16).astype(np.uint32) << 16).view(np.float32)
+
+
+class MixedRows:
+    """Tables in the BF16 storage form: FP32 rows 0..n_hot-1, BF16 bits after."""
+
+    def __init__(self, full, vocab_size, dim, n_hot):
+        full = np.ascontiguousarray(full, np.float32)
+        self.dim, self.n_hot = dim, n_hot
+        self.f32 = full[: n_hot * dim].copy()
+        self.bf = bf16_rne(full[n_hot * dim:])
+
+    def full(self):
+        return np.concatenate([self.f32, bf16_to_f32(self.bf)])
+
+
+def round_sr_seed(seed, round_):
+    return lib().orc_round_sr_seed(seed, round_)
+
+
+def skipgram_bf16(m0, m1, sr_seed, exp_tab, table, vocab_size, sen, sent_start, first, n, window, dim,
+                  negative, alpha, cbow=False):
+    fn = lib().orc_cbow_bf16 if cbow else lib().orc_skipgram_bf16
+    fn(ptr(m0.f32, f32p), ptr(m0.bf, u16p), ptr(m1.f32, f32p), ptr(m1.bf, u16p), m0.n_hot, sr_seed,
+       ptr(exp_tab, f32p), ptr(table, i32p), len(table), vocab_size,
        ptr(np.ascontiguousarray(sen, np.int32), i32p), ptr(np.ascontiguousarray(sent_start, np.uint64), u64p),
        first, n, window, dim, negative, alpha)
 
