@@ -19,6 +19,7 @@
 #include "budget.cuh"
 #include "common.cuh"
 #include "graph.cuh"
+#include "pairs.cuh"
 #include "plan.cuh"
 #include "sgns.cuh"
 #include "walk.cuh"
@@ -28,6 +29,7 @@ using namespace felog;
 namespace {
 
 constexpr int64_t kTableSize = 100000000;  // table_size, word2vec.cu:171
+constexpr uint64_t kPairChunk = 1ull << 27;  // pair records generated and trained per chunk
 
 template <class T>
 struct DevBuf {
@@ -118,6 +120,12 @@ struct felog_ctx {
   DevBuf<unsigned long long> p_state, p_neg_state;
   DevBuf<uint64_t> p_out_off, p_batch_first;
   DevBuf<int32_t> p_sen, p_negs;
+  DevBuf<uint64_t> pr_count, pr_off;  // pair stream: pairs per sentence, offsets
+  DevBuf<int32_t> pr_rec;             // pair stream records
+  DevBuf<unsigned long long> pr_cstate, pr_jump;
+  DevBuf<uint32_t> pr_cfirst;
+  int pr_jump_window = -1, pr_jump_k = -1;
+  std::vector<uint64_t> h_pr_off;
   uint64_t plan_sent = 0, plan_sen = 0, plan_batches = 0;
 
   // budget
@@ -270,7 +278,7 @@ extern "C" void felog_destroy(felog_ctx *c) {
   c->exp_table.release(); c->syn0.release(); c->syn1.release(); c->syn0_bf.release(); c->syn1_bf.release(); c->jump.release();
   c->p_cand.release(); c->p_draws.release(); c->p_cons.release(); c->p_kept.release(); c->p_blk.release();
   c->p_state.release(); c->p_neg_state.release(); c->p_out_off.release(); c->p_batch_first.release();
-  c->p_sen.release(); c->p_negs.release(); c->sim.release(); c->cub_tmp.release(); c->out_tmp.release();
+  c->p_sen.release(); c->pr_count.release(); c->pr_off.release(); c->pr_rec.release(); c->pr_cstate.release(); c->pr_jump.release(); c->pr_cfirst.release(); c->p_negs.release(); c->sim.release(); c->cub_tmp.release(); c->out_tmp.release();
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
   if (c->tm0) cudaEventDestroy(c->tm0);
@@ -928,8 +936,6 @@ felog_status plan_round(felog_ctx *c, float *ms) {
 template <int D, class P>
 void launch_dim(felog_ctx *c, const SgArgs &g, int blocks, int threads) {
   if (c->o.cbow) k_sgns_cbow<D, P><<<blocks, threads, 0, c->stream>>>(g);
-  else if (c->o.negative == 5) k_sgns_skipgram<D, 5, P><<<blocks, threads, 0, c->stream>>>(g);
-  else if (c->o.negative == 7) k_sgns_skipgram<D, 7, P><<<blocks, threads, 0, c->stream>>>(g);
   else k_sgns_skipgram_any<D, P><<<blocks, threads, 0, c->stream>>>(g);
 }
 
@@ -941,6 +947,123 @@ void launch_trainer(felog_ctx *c, const SgArgs &g, int blocks, int threads) {
     case 128: launch_dim<128, P>(c, g, blocks, threads); break;
     case 256: launch_dim<256, P>(c, g, blocks, threads); break;
   }
+}
+
+template <int D, int K, class P>
+void launch_pairs_dkp(felog_ctx *c, const SgArgs &g, int blocks, int threads, uint64_t base, uint64_t s0) {
+  k_sgns_train_pairs<D, K, P><<<blocks, threads, 0, c->stream>>>(g, c->pr_rec.p, c->pr_off.p, base, s0);
+}
+
+template <int K, class P>
+void launch_pairs_kp(felog_ctx *c, const SgArgs &g, int blocks, int threads, uint64_t base, uint64_t s0) {
+  switch (c->o.size) {
+    case 64: launch_pairs_dkp<64, K, P>(c, g, blocks, threads, base, s0); break;
+    case 128: launch_pairs_dkp<128, K, P>(c, g, blocks, threads, base, s0); break;
+    case 256: launch_pairs_dkp<256, K, P>(c, g, blocks, threads, base, s0); break;
+  }
+}
+
+// Skip-gram with K = 5 or 7 over the pair stream: count the pairs of every
+// sentence, scan, then per chunk of at most kPairChunk pairs emit the records
+// and train them.
+felog_status train_pairs(felog_ctx *c, SgArgs g, int blocks, int threads) {
+  const uint64_t n = c->plan_sent;
+  const int K = c->o.negative;
+  const int stride = pair_stride(K);
+  CK(c->pr_count.ensure(n + 1), "train: pair counts");
+  CK(c->pr_off.ensure(n + 1), "train: pair offsets");
+  PairArgs pa{};
+  pa.sen = c->p_sen.p;
+  pa.sent_start = c->p_out_off.p;
+  pa.blk = c->p_blk.p;
+  pa.s0 = 0;
+  pa.s1 = n;
+  pa.table = c->table.p;
+  pa.fm_window = g.fm_window;
+  pa.fm_vocab1 = g.fm_vocab1;
+  pa.window = c->o.window;
+  pa.negative = K;
+  pa.stride = stride;
+  // the negative LCG advanced by K j steps, j = 0 .. 2 window
+  const int nj = 2 * c->o.window + 1;
+  if (c->pr_jump_window != c->o.window || c->pr_jump_k != K) {
+    std::vector<unsigned long long> jt(2 * (size_t)nj);
+    unsigned long long A = 1, C = 0;
+    for (int j = 0; j < nj; j++) {
+      jt[j] = A;
+      jt[nj + j] = C;
+      A = A * g.lcg_a[K - 1];
+      C = C * g.lcg_a[K - 1] + g.lcg_c[K - 1];
+    }
+    CK(c->pr_jump.ensure(2 * (size_t)nj), "train: jump table");
+    CK(cudaMemcpy(c->pr_jump.p, jt.data(), 8 * jt.size(), cudaMemcpyHostToDevice), "train: jump table");
+    c->pr_jump_window = c->o.window;
+    c->pr_jump_k = K;
+  }
+  pa.jump_a = c->pr_jump.p;
+  pa.jump_c = c->pr_jump.p + nj;
+  CK(c->pr_cstate.ensure(c->plan_sen + 1), "train: center states");
+  CK(c->pr_cfirst.ensure(c->plan_sen + 1), "train: center offsets");
+  pa.cstate = c->pr_cstate.p;
+  pa.cfirst = c->pr_cfirst.p;
+  pa.count = c->pr_count.p;
+  pa.off = c->pr_off.p;
+  CK(cudaMemsetAsync(c->pr_count.p + n, 0, 8, c->stream), "train");
+  if (n) {
+    k_pair_count<<<grid_for(c, n, 256), 256, 0, c->stream>>>(pa);
+    c->launches++;
+  }
+  size_t tmp = 0;
+  CK(cub::DeviceScan::ExclusiveSum(nullptr, tmp, c->pr_count.p, c->pr_off.p, (int)(n + 1), c->stream), "train");
+  CK(c->cub_tmp.ensure(tmp), "train");
+  CK(cub::DeviceScan::ExclusiveSum(c->cub_tmp.p, tmp, c->pr_count.p, c->pr_off.p, (int)(n + 1), c->stream),
+     "train");
+  uint64_t total = 0;
+  CK(cudaMemcpyAsync(&total, c->pr_off.p + n, 8, cudaMemcpyDeviceToHost, c->stream), "train");
+  CK(cudaStreamSynchronize(c->stream), "train");
+  // chunks of whole sentences
+  std::vector<std::pair<uint64_t, uint64_t>> chunks;
+  if (total <= kPairChunk) {
+    chunks.push_back({0, n});
+  } else {
+    c->h_pr_off.resize(n + 1);
+    CK(cudaMemcpy(c->h_pr_off.data(), c->pr_off.p, 8 * (n + 1), cudaMemcpyDeviceToHost), "train");
+    uint64_t s0 = 0;
+    while (s0 < n) {
+      uint64_t s1 = s0 + 1;
+      while (s1 < n && c->h_pr_off[s1 + 1] - c->h_pr_off[s0] <= kPairChunk) s1++;
+      chunks.push_back({s0, s1});
+      s0 = s1;
+    }
+  }
+  const uint64_t cap = std::min<uint64_t>(total, kPairChunk) + 1;
+  uint64_t need = cap;
+  for (auto &ch : chunks)
+    if (total > kPairChunk) need = std::max<uint64_t>(need, c->h_pr_off[ch.second] - c->h_pr_off[ch.first] + 1);
+  CK(c->pr_rec.ensure(need * stride), "train: pair records");
+  pa.rec = c->pr_rec.p;
+  const bool bf = c->o.precision == FELOG_BF16;
+  for (auto &ch : chunks) {
+    pa.s0 = ch.first;
+    pa.s1 = ch.second;
+    pa.base = total > kPairChunk ? c->h_pr_off[ch.first] : 0;
+    const int eb = grid_for(c, (ch.second - ch.first) * 32, 256);
+    if (K == 5) k_pair_emit<5><<<eb, 256, 0, c->stream>>>(pa);
+    else k_pair_emit<7><<<eb, 256, 0, c->stream>>>(pa);
+    c->launches++;
+    CK(cudaMemsetAsync(c->counters.p + 0, 0, 8, c->stream), "train");  // sentence claim counter
+    g.n_sent = ch.second - ch.first;
+    if (K == 5) {
+      if (bf) launch_pairs_kp<5, RowsBF16>(c, g, blocks, threads, pa.base, pa.s0);
+      else launch_pairs_kp<5, RowsF32>(c, g, blocks, threads, pa.base, pa.s0);
+    } else {
+      if (bf) launch_pairs_kp<7, RowsBF16>(c, g, blocks, threads, pa.base, pa.s0);
+      else launch_pairs_kp<7, RowsF32>(c, g, blocks, threads, pa.base, pa.s0);
+    }
+    c->launches++;
+    CK(cudaGetLastError(), "train_round: launch");
+  }
+  return FELOG_OK;
 }
 
 }  // namespace
@@ -994,10 +1117,15 @@ extern "C" felog_status felog_train_round(felog_ctx *c, uint32_t round, float al
   const int blocks = c->o.deterministic ? 1 : c->sm_count * 8;
   const int threads = c->o.deterministic ? 32 : 256;
   CK(cudaEventRecord(c->ev0, c->stream), "train_round");
-  if (c->o.precision == FELOG_BF16) launch_trainer<RowsBF16>(c, g, blocks, threads);
-  else launch_trainer<RowsF32>(c, g, blocks, threads);
-  c->launches++;
-  CK(cudaGetLastError(), "train_round: launch");
+  if (!c->o.cbow && c->o.size >= 64 && (c->o.negative == 5 || c->o.negative == 7)) {
+    s = train_pairs(c, g, blocks, threads);
+    if (s != FELOG_OK) return s;
+  } else {
+    if (c->o.precision == FELOG_BF16) launch_trainer<RowsBF16>(c, g, blocks, threads);
+    else launch_trainer<RowsF32>(c, g, blocks, threads);
+    c->launches++;
+    CK(cudaGetLastError(), "train_round: launch");
+  }
   CK(cudaEventRecord(c->ev1, c->stream), "train_round");
   unsigned long long h[4];
   CK(cudaMemcpyAsync(h, c->counters.p, sizeof h, cudaMemcpyDeviceToHost, c->stream), "train_round");

@@ -1,0 +1,451 @@
+// Pair stream of one skip-gram round: for every (center, context) pair of the
+// batch plan, in the reference's draw order, the context row, the positive
+// target (the center word) and the K negative targets of skip_gram_kernel
+// (word2vec.cu:442-536, hs = 0):
+//   per center (in sentence order): next = next * 2514903917 + 11,
+//     b = next % window (the window shrink, :458-459);
+//   per context a in [b, 2 window + 1 - b), a != window, inside the sentence:
+//     K draws next = next * 25214903917 + 11, target = table[(next >> 16) %
+//     1e8], 0 -> next % (vocab - 1) + 1, skipped when equal to the word
+//     (:496-507);
+// with next seeded by the sentence's index in its batch (blockIdx.x, :446).
+// The draws depend only on the plan, never on the rows, so one scalar thread
+// per sentence produces them ahead of training; the trainer's warps then do
+// row work only.
+//
+// Record of one pair (int32 x stride, stride = K + 3 rounded up to 4):
+//   [0] context row, [1] positive target, [2 .. K+1] negatives (-1: skipped),
+//   [K+2] flags: bit 0 = two non-skipped negatives hit the same row.
+#pragma once
+
+#include "common.cuh"
+#include "sgns.cuh"
+
+namespace felog {
+
+constexpr uint32_t kPairDup = 1u;
+
+__host__ __device__ constexpr int pair_stride(int negative) { return (negative + 3 + 3) & ~3; }
+
+struct PairArgs {
+  const int32_t *sen;
+  const uint64_t *sent_start;  // plan sentence starts (n_sent + 1)
+  const uint32_t *blk;         // index of each sentence in its batch
+  uint64_t s0, s1;             // sentences of this chunk
+  const int32_t *table;
+  FastMod fm_window;
+  FastMod fm_vocab1;
+  int window;
+  int negative;
+  int stride;
+  uint64_t *count;       // pairs per sentence (count kernel: sentences s0..s1)
+  const uint64_t *off;   // exclusive scan of count over the round's sentences
+  uint64_t base;         // off[s0]: the first pair of the chunk
+  int32_t *rec;          // records of the chunk (pair off[s] - base at rec + (off[s] - base) * stride)
+  unsigned long long *cstate;  // per center (plan token): LCG state after its window draw
+  uint32_t *cfirst;            // per center: pairs of its sentence before it
+  const unsigned long long *jump_a, *jump_c;  // the negative LCG advanced by K j steps, j < 2 window
+};
+
+// number of valid contexts of the center at pos with window shrink b
+__device__ __forceinline__ int contexts_of(long long pos, long long sb, long long se, int window, int b) {
+  long long lo = pos - window + b, hi = pos + window - b;  // inclusive context positions
+  if (lo < sb) lo = sb;
+  if (hi > se - 1) hi = se - 1;
+  if (hi < lo) return 0;
+  return (int)(hi - lo + 1) - 1;  // minus the center itself (always inside)
+}
+
+__global__ void k_pair_count(PairArgs a) {
+  for (uint64_t s = a.s0 + blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; s < a.s1;
+       s += (uint64_t)gridDim.x * blockDim.x) {
+    const long long sb = (long long)a.sent_start[s], se = (long long)a.sent_start[s + 1];
+    unsigned long long nr = a.blk[s];
+    uint64_t n = 0;
+    for (long long pos = sb; pos < se; pos++) {
+      nr = nr * 2514903917ULL + 11ULL;
+      const int b = (int)fastmod(nr, a.fm_window);
+      const int c = contexts_of(pos, sb, se, a.window, b);
+      a.cstate[pos] = nr;
+      a.cfirst[pos] = (uint32_t)n;
+      n += (uint64_t)c;
+      if (c) nr = a.jump_a[c] * nr + a.jump_c[c];
+    }
+    a.count[s] = n;
+  }
+}
+
+// One warp per sentence; lane i expands pairs p0 + i + 32 u (u < kEmitUnroll,
+// interleaved so that their table loads are in flight together).  A pair's
+// center is the last one whose first pair is <= p, its context the
+// (p - first)-th valid window position, and its K draws start from the
+// center's post-window state advanced by K (p - first) steps.  Lanes write
+// consecutive records (coalesced).
+constexpr int kEmitUnroll = 4;
+
+template <int K>
+__global__ void __launch_bounds__(256) k_pair_emit(PairArgs a) {
+  constexpr int S = pair_stride(K);
+  constexpr int U = kEmitUnroll;
+  const int lane = lane_id();
+  const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarps = (gridDim.x * (uint64_t)blockDim.x) >> 5;
+  for (uint64_t s = a.s0 + warp; s < a.s1; s += nwarps) {
+    const long long sb = (long long)a.sent_start[s], se = (long long)a.sent_start[s + 1];
+    const uint64_t np = a.off[s + 1] - a.off[s];
+    int32_t *r0 = a.rec + (a.off[s] - a.base) * (uint64_t)S;
+    for (uint64_t p0 = 0; p0 < np; p0 += 32 * U) {
+      long long pos[U], lo[U], hi[U];
+      bool live[U];
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        live[u] = p0 + lane + 32 * u < np;
+        lo[u] = sb;
+        hi[u] = se - 1;
+      }
+      // centers: largest pos in [sb, se) with cfirst[pos] <= p (binary searches side by side)
+      while (true) {
+        bool any = false;
+#pragma unroll
+        for (int u = 0; u < U; u++) any |= lo[u] < hi[u];
+        if (!any) break;
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+          if (lo[u] < hi[u]) {
+            const long long mid = (lo[u] + hi[u] + 1) >> 1;
+            if ((uint64_t)a.cfirst[mid] <= p0 + lane + 32 * u) lo[u] = mid;
+            else hi[u] = mid - 1;
+          }
+        }
+      }
+      unsigned long long nr[U];
+      int word[U], ctx[U];
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        pos[u] = lo[u];
+        const uint64_t p = p0 + lane + 32 * u;
+        const uint32_t j = live[u] ? (uint32_t)(p - a.cfirst[pos[u]]) : 0u;
+        nr[u] = a.cstate[pos[u]];
+        const int b = (int)fastmod(nr[u], a.fm_window);
+        long long c = pos[u] - a.window + b;
+        if (c < sb) c = sb;
+        c += j;
+        if (c >= pos[u]) c++;
+        if (c >= se) c = se - 1;  // only for lanes past the end (not written)
+        word[u] = a.sen[pos[u]];
+        ctx[u] = a.sen[c];
+        nr[u] = a.jump_a[j] * nr[u] + a.jump_c[j];
+      }
+      int32_t t[U][K];
+#pragma unroll
+      for (int q = 0; q < K; q++)
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+          nr[u] = nr[u] * 25214903917ULL + 11ULL;
+          t[u][q] = __ldg(&a.table[(nr[u] >> 16) % kUnigramSlots]);
+          if (t[u][q] == 0) t[u][q] = -2 - (int)fastmod(nr[u], a.fm_vocab1);  // fallback, resolved below
+        }
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        if (!live[u]) continue;
+        uint32_t flags = 0;
+        int32_t rv[S];
+        rv[0] = ctx[u];
+        rv[1] = word[u];
+#pragma unroll
+        for (int q = 0; q < K; q++) {
+          int v = t[u][q];
+          if (v < 0) v = -2 - v + 1;  // next % (vocab - 1) + 1
+          v = v == word[u] ? -1 : v;
+#pragma unroll
+          for (int q2 = 0; q2 < q; q2++) flags |= (v >= 0 && rv[2 + q2] == v) ? kPairDup : 0u;
+          rv[2 + q] = v;
+        }
+        rv[2 + K] = (int32_t)flags;
+#pragma unroll
+        for (int q = K + 3; q < S; q++) rv[q] = 0;
+        int4 *dst = reinterpret_cast<int4 *>(r0 + (p0 + lane + 32 * u) * S);
+#pragma unroll
+        for (int k = 0; k < S / 4; k++) dst[k] = make_int4(rv[4 * k], rv[4 * k + 1], rv[4 * k + 2], rv[4 * k + 3]);
+      }
+    }
+  }
+}
+
+// ---- row access for the pair trainer (DIM >= 64, J = DIM / 32 >= 2): each
+// lane's J values as J / 2 float2, so the elementwise work runs on the packed
+// FP32 pipe (one instruction per two values, each value rounded as in the
+// scalar form).
+template <int DIM, class P>
+struct LaneRows {
+  static constexpr int J = DIM / 32;
+  static constexpr int H = J / 2;
+  const float *f[2];     // FP32 rows of syn0 / syn1 with this lane's offset
+  const uint16_t *b[2];  // BF16 rows with this lane's offset, shifted so row r is at b + r * DIM
+  uint32_t n_hot;
+
+  __device__ __forceinline__ void init(const SgArgs &a) {
+    const int lo = lane_id() * J;
+    f[0] = a.syn0 + lo;
+    f[1] = a.syn1 + lo;
+    n_hot = 0;
+    b[0] = b[1] = nullptr;
+    if constexpr (P::kBF16) {
+      n_hot = (uint32_t)a.n_hot;
+      const uintptr_t shift = (uintptr_t)a.n_hot * DIM * sizeof(uint16_t);
+      b[0] = reinterpret_cast<const uint16_t *>(reinterpret_cast<uintptr_t>(a.syn0_bf + lo) - shift);
+      b[1] = reinterpret_cast<const uint16_t *>(reinterpret_cast<uintptr_t>(a.syn1_bf + lo) - shift);
+    }
+  }
+
+  template <int W>
+  __device__ __forceinline__ void load(uint32_t row, float2 (&r)[H]) const {
+    const float *pf = f[W] + (size_t)row * DIM;
+    if constexpr (!P::kBF16) {
+      load_f32(pf, r);
+    } else {
+      const bool hot = row < n_hot;
+      const uint16_t *pb = b[W] + (size_t)row * DIM;
+      float2 fv[H];
+      uint32_t hv[H];
+#pragma unroll
+      for (int k = 0; k < H; k++) {
+        fv[k] = make_float2(0.0f, 0.0f);
+        hv[k] = 0u;
+      }
+      if (hot) load_f32(pf, fv);
+      else load_b16(pb, hv);
+#pragma unroll
+      for (int k = 0; k < H; k++) r[k] = hot ? fv[k] : make_float2(bf16_lo(hv[k]), bf16_hi(hv[k]));
+    }
+  }
+
+  // row += u.  FP32 rows: vector reduction (cur unchanged, returns false).
+  // BF16 rows: cur becomes SR(cur + u), stored with a plain store (returns true).
+  template <int W>
+  __device__ __forceinline__ bool update(uint32_t row, const float2 (&u)[H], float2 (&cur)[H],
+                                         uint32_t stream) const {
+    float *pf = const_cast<float *>(f[W]) + (size_t)row * DIM;
+    if constexpr (!P::kBF16) {
+      red_f32x2(pf, u);
+      return false;
+    } else {
+      const bool hot = row < n_hot;
+      uint32_t w[H];
+#pragma unroll
+      for (int k = 0; k < H; k++) {
+        const float2 nv = __fadd2_rn(cur[k], u[k]);
+        w[k] = sr_bf16x2(nv.y, nv.x, sr_word(stream));
+      }
+      if (hot) {
+        red_f32x2(pf, u);
+      } else {
+        store_b16(const_cast<uint16_t *>(b[W]) + (size_t)row * DIM, w);
+#pragma unroll
+        for (int k = 0; k < H; k++) cur[k] = make_float2(bf16_lo(w[k]), bf16_hi(w[k]));
+      }
+      return !hot;
+    }
+  }
+
+  static __device__ __forceinline__ void load_f32(const float *p, float2 (&r)[H]) {
+    if constexpr (H % 2 == 0) {
+#pragma unroll
+      for (int k = 0; k < H / 2; k++) {
+        const float4 v = __ldcg(reinterpret_cast<const float4 *>(p) + k);
+        r[2 * k] = make_float2(v.x, v.y);
+        r[2 * k + 1] = make_float2(v.z, v.w);
+      }
+    } else {
+      r[0] = __ldcg(reinterpret_cast<const float2 *>(p));
+    }
+  }
+  static __device__ __forceinline__ void load_b16(const uint16_t *p, uint32_t (&h)[H]) {
+    if constexpr (H == 4) {
+      const uint4 v = __ldcg(reinterpret_cast<const uint4 *>(p));
+      h[0] = v.x; h[1] = v.y; h[2] = v.z; h[3] = v.w;
+    } else if constexpr (H == 2) {
+      const uint2 v = __ldcg(reinterpret_cast<const uint2 *>(p));
+      h[0] = v.x; h[1] = v.y;
+    } else {
+      h[0] = __ldcg(reinterpret_cast<const unsigned int *>(p));
+    }
+  }
+  static __device__ __forceinline__ void store_b16(uint16_t *p, const uint32_t (&w)[H]) {
+    if constexpr (H == 4) *reinterpret_cast<uint4 *>(p) = make_uint4(w[0], w[1], w[2], w[3]);
+    else if constexpr (H == 2) *reinterpret_cast<uint2 *>(p) = make_uint2(w[0], w[1]);
+    else *reinterpret_cast<unsigned int *>(p) = w[0];
+  }
+  static __device__ __forceinline__ void red_f32x2(float *p, const float2 (&u)[H]) {
+    if constexpr (H % 2 == 0) {
+#pragma unroll
+      for (int k = 0; k < H / 2; k++) red_add_v4(p + 4 * k, u[2 * k].x, u[2 * k].y, u[2 * k + 1].x, u[2 * k + 1].y);
+    } else {
+      red_add_v2(p, u[0].x, u[0].y);
+    }
+  }
+};
+
+// in-lane part of the reference tree (pair t with t + DIM/2 via a*b + c, then
+// halve) on packed values; lane value j is element j % 2 of pair j / 2
+template <int H>
+__device__ __forceinline__ float fold2(const float2 (&x)[H], const float2 (&y)[H]) {
+  if constexpr (H == 1) {
+    return __fmaf_rn(x[0].y, y[0].y, __fmul_rn(x[0].x, y[0].x));
+  } else {
+    float2 s[H / 2];
+#pragma unroll
+    for (int k = 0; k < H / 2; k++) s[k] = __ffma2_rn(x[k + H / 2], y[k + H / 2], __fmul2_rn(x[k], y[k]));
+#pragma unroll
+    for (int h = H / 4; h >= 1; h >>= 1)
+#pragma unroll
+      for (int k = 0; k < h; k++) s[k] = __fadd2_rn(s[k], s[k + h]);
+    return __fadd_rn(s[0].x, s[0].y);
+  }
+}
+
+template <int H>
+__device__ __forceinline__ float sg_dot2(const float2 (&x)[H], const float2 (&y)[H]) {
+  float r = fold2<H>(x, y);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) r = __fadd_rn(r, __shfl_xor_sync(0xffffffffu, r, o));
+  return r;
+}
+
+// multi_dot on packed values: the same butterfly over the in-lane folds
+template <int H, int NT>
+__device__ __forceinline__ float multi_dot2(const float2 (&x)[H], const float2 (&y)[NT][H]) {
+  static_assert(NT <= 8, "up to 8 targets");
+  const int lane = lane_id();
+  float v[8];
+#pragma unroll
+  for (int q = 0; q < 8; q++) v[q] = q < NT ? fold2<H>(x, y[q]) : 0.0f;
+  const bool b4 = lane & 16, b3 = lane & 8, b2 = lane & 4;
+  float w[4];
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    const float keep = b4 ? v[k + 4] : v[k], send = b4 ? v[k] : v[k + 4];
+    w[k] = __fadd_rn(keep, __shfl_xor_sync(0xffffffffu, send, 16));
+  }
+  float u[2];
+#pragma unroll
+  for (int k = 0; k < 2; k++) {
+    const float keep = b3 ? w[k + 2] : w[k], send = b3 ? w[k] : w[k + 2];
+    u[k] = __fadd_rn(keep, __shfl_xor_sync(0xffffffffu, send, 8));
+  }
+  float z = __fadd_rn(b2 ? u[1] : u[0], __shfl_xor_sync(0xffffffffu, b2 ? u[0] : u[1], 4));
+  z = __fadd_rn(z, __shfl_xor_sync(0xffffffffu, z, 2));
+  z = __fadd_rn(z, __shfl_xor_sync(0xffffffffu, z, 1));
+  return z;
+}
+
+template <int S>
+__device__ __forceinline__ int rec_at(const int4 (&v)[S / 4], int i) {
+  const int4 q = v[i / 4];
+  return (i & 3) == 0 ? q.x : (i & 3) == 1 ? q.y : (i & 3) == 2 ? q.z : q.w;
+}
+
+// skip_gram_kernel semantics (word2vec.cu:442-536, hs = 0) over the pair
+// stream: one warp per sentence, the sentence's pairs in order.  The record of
+// the next pair is loaded one pair ahead (every lane reads the same 16-byte
+// words: one broadcast request).  With distinct targets the K + 1 scores come
+// from one multi_dot and each lane evaluates one gradient; a pair whose
+// negatives repeat a row takes the sequential path, where the later target
+// sees the earlier update as in the reference.
+template <int DIM, int NK, class P>
+__global__ void __launch_bounds__(256, DIM >= 256 ? 2 : 4)
+    k_sgns_train_pairs(SgArgs a, const int32_t *__restrict__ rec, const uint64_t *__restrict__ off, uint64_t base,
+                       uint64_t s0) {
+  static_assert(DIM >= 64, "two or more values per lane");
+  constexpr int H = DIM / 64;
+  constexpr int NT = NK + 1;
+  constexpr int S = pair_stride(NK);
+  constexpr bool kMulti = NT <= 8;
+  __shared__ float s_exp[1000];
+  load_exp(a, s_exp);
+  const int lane = lane_id();
+  LaneRows<DIM, P> rows;
+  rows.init(a);
+  unsigned long long my_pairs = 0;
+  unsigned long long sc;
+  while (claim_sentence(a, sc)) {
+    const uint64_t gs = s0 + sc;  // sentence index in the round's plan
+    const uint64_t pb = off[gs] - base, pe = off[gs + 1] - base;
+    if (pb == pe) continue;
+    int4 nxt[S / 4];
+#pragma unroll
+    for (int k = 0; k < S / 4; k++) nxt[k] = __ldg(reinterpret_cast<const int4 *>(rec + pb * S) + k);
+    for (uint64_t p = pb; p < pe; p++) {
+      int4 cur[S / 4];
+#pragma unroll
+      for (int k = 0; k < S / 4; k++) cur[k] = nxt[k];
+      if (p + 1 < pe) {
+#pragma unroll
+        for (int k = 0; k < S / 4; k++) nxt[k] = __ldg(reinterpret_cast<const int4 *>(rec + (p + 1) * S) + k);
+      }
+      const uint32_t l1 = (uint32_t)rec_at<S>(cur, 0);
+      int tg[NT];
+#pragma unroll
+      for (int q = 0; q < NT; q++) tg[q] = rec_at<S>(cur, 1 + q);
+      const bool dup = (rec_at<S>(cur, NK + 2) & kPairDup) != 0;
+      float2 x[H];
+      rows.template load<0>(l1, x);
+      float2 y[NT][H];
+#pragma unroll
+      for (int q = 0; q < NT; q++)
+        if (tg[q] >= 0) rows.template load<1>((uint32_t)tg[q], y[q]);
+      float2 neu[H];
+#pragma unroll
+      for (int k = 0; k < H; k++) neu[k] = make_float2(0.0f, 0.0f);
+      const uint32_t key = P::kBF16 ? lane_key(a.sr_seed, gs, (uint32_t)(p - pb), lane) : 0u;
+      bool done = false;
+      if constexpr (kMulti) {
+        if (!dup) {
+          const float z = multi_dot2<H, NT>(x, y);
+          const int tq = butterfly_target(lane);
+          const float gv = tq < NT ? sg_grad(z, tq == 0 ? 1 : 0, s_exp, a.alpha) : 0.0f;
+#pragma unroll
+          for (int q = 0; q < NT; q++) {
+            const float g = __shfl_sync(0xffffffffu, gv, butterfly_lane(q));
+            if (tg[q] < 0) continue;
+            const float2 g2 = make_float2(g, g);
+            float2 upd[H];
+#pragma unroll
+            for (int k = 0; k < H; k++) {
+              neu[k] = __ffma2_rn(g2, y[q][k], neu[k]);
+              upd[k] = __fmul2_rn(g2, x[k]);
+            }
+            rows.template update<1>((uint32_t)tg[q], upd, y[q], slot_stream(key, q));
+          }
+          done = true;
+        }
+      }
+      if (!done) {
+#pragma unroll
+        for (int q = 0; q < NT; q++) {
+          if (tg[q] < 0) continue;
+          const float f = sg_dot2<H>(x, y[q]);
+          const float g = sg_grad(f, q == 0 ? 1 : 0, s_exp, a.alpha);
+          const float2 g2 = make_float2(g, g);
+          float2 upd[H];
+#pragma unroll
+          for (int k = 0; k < H; k++) {
+            neu[k] = __ffma2_rn(g2, y[q][k], neu[k]);
+            upd[k] = __fmul2_rn(g2, x[k]);
+          }
+          const bool stored = rows.template update<1>((uint32_t)tg[q], upd, y[q], slot_stream(key, q));
+#pragma unroll
+          for (int r = q + 1; r < NT; r++)
+            if (tg[r] == tg[q])
+#pragma unroll
+              for (int k = 0; k < H; k++) y[r][k] = stored ? y[q][k] : __fadd2_rn(y[q][k], upd[k]);
+        }
+      }
+      rows.template update<0>(l1, neu, x, slot_stream(key, kSlotCtx));
+      my_pairs++;
+    }
+  }
+  if (lane == 0 && my_pairs) atomicAdd(a.pairs, my_pairs);
+}
+
+}  // namespace felog

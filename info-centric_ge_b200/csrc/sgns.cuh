@@ -420,147 +420,6 @@ __global__ void __launch_bounds__(256) k_sgns_skipgram_any(SgArgs a) {
   if (lane_id() == 0 && my_pairs) atomicAdd(a.pairs, my_pairs);
 }
 
-// skip_gram_kernel semantics for a fixed number of negatives NK, pipelined.
-// The draw sequence of the reference's LCG does not depend on the rows, so the
-// next (center, context) pair and its unigram-table slots are produced while
-// the current pair trains: the next pair's table loads are in flight during
-// the current pair's row loads and updates.  Lane q < NK computes negative q
-// directly: the LCG state after q + 1 steps is an affine map of the state
-// before the pair's draws (lcg_a, lcg_c), so the K draws of the reference's
-// loop (:502-505) cost one multiply-add per lane; the window draw (:458-459)
-// stays one step per center.  With distinct targets the K + 1 scores come
-// from one multi_dot and each lane evaluates one gradient; a pair whose
-// targets repeat a row takes the sequential path, where the later target sees
-// the earlier update as in the reference.
-template <int DIM, int NK, class P>
-__global__ void __launch_bounds__(256, DIM >= 256 ? 2 : 4) k_sgns_skipgram(SgArgs a) {
-  constexpr int J = DIM / 32;
-  constexpr int NT = NK + 1;
-  constexpr bool kMulti = J >= 2 && NT <= 8;
-  static_assert(NK < 32, "one lane per negative");
-  __shared__ float s_exp[1000];
-  load_exp(a, s_exp);
-  const int lane = lane_id();
-  const unsigned long long my_a = lane < NK ? a.lcg_a[lane] : 0ULL;
-  const unsigned long long my_c = lane < NK ? a.lcg_c[lane] : 0ULL;
-  unsigned long long my_pairs = 0;
-  unsigned long long s;
-  while (claim_sentence(a, s)) {
-    const long long sb = (long long)a.sent_start[s], se = (long long)a.sent_start[s + 1];
-    unsigned long long nr = a.blk[s];
-    long long pos = sb - 1;
-    int aa = 0, hi = 0, word = 0;
-    // next valid pair: center word, context row, and this lane's negative
-    auto advance = [&](int &w_out, int &l1_out, int &t_lane) -> bool {
-      for (;;) {
-        if (aa >= hi) {
-          pos++;
-          if (pos >= se) return false;
-          word = __ldg(&a.sen[pos]);
-          nr = nr * 2514903917ULL + 11ULL;
-          const int b = (int)fastmod(nr, a.fm_window);
-          aa = b;
-          hi = a.window * 2 + 1 - b;
-        }
-        const int ca = aa++;
-        if (ca == a.window) continue;
-        const long long c = pos - a.window + ca;
-        if (c < sb || c >= se) continue;
-        w_out = word;
-        l1_out = __ldg(&a.sen[c]);
-        unsigned long long sq = 0;
-        t_lane = 0;
-        if (lane < NK) {
-          sq = my_a * nr + my_c;
-          const int32_t tv = __ldg(&a.table[(sq >> 16) % kUnigramSlots]);
-          t_lane = tv == 0 ? (int)fastmod(sq, a.fm_vocab1) + 1 : tv;
-        }
-        nr = __shfl_sync(0xffffffffu, sq, NK - 1);  // state after the K draws
-        return true;
-      }
-    };
-    int c_word = 0, c_l1 = 0, c_t = 0;
-    uint32_t pair = 0;
-    bool have = advance(c_word, c_l1, c_t);
-    while (have) {
-      int n_word = 0, n_l1 = 0, n_t = 0;
-      const bool nhave = advance(n_word, n_l1, n_t);
-      // targets of the current pair (word2vec.cu:496-507); -1: negative equal to the word
-      int tg[NT];
-      tg[0] = c_word;
-#pragma unroll
-      for (int q = 0; q < NK; q++) {
-        const int t = __shfl_sync(0xffffffffu, c_t, q);
-        tg[q + 1] = t == c_word ? -1 : t;
-      }
-      bool dup = false;
-#pragma unroll
-      for (int q = 2; q < NT; q++)
-#pragma unroll
-        for (int r = 1; r < q; r++) dup |= tg[q] >= 0 && tg[q] == tg[r];
-      float x[J];
-      row_load<DIM, P>(a, 0, c_l1, x);
-      float y[NT][J];
-#pragma unroll
-      for (int q = 0; q < NT; q++)
-        if (tg[q] >= 0) row_load<DIM, P>(a, 1, tg[q], y[q]);
-      float neu[J];
-#pragma unroll
-      for (int j = 0; j < J; j++) neu[j] = 0.0f;
-      const uint32_t key = P::kBF16 ? lane_key(a.sr_seed, s, pair, lane_id()) : 0u;
-      bool done = false;
-      if constexpr (kMulti) {
-        if (!dup) {
-          const float z = multi_dot<J, NT>(x, y);
-          const int tq = butterfly_target(lane);
-          const float gv = tq < NT ? sg_grad(z, tq == 0 ? 1 : 0, s_exp, a.alpha) : 0.0f;
-#pragma unroll
-          for (int q = 0; q < NT; q++) {
-            const float g = __shfl_sync(0xffffffffu, gv, butterfly_lane(q));
-            if (tg[q] < 0) continue;
-            float upd[J];
-#pragma unroll
-            for (int j = 0; j < J; j++) {
-              neu[j] = __fmaf_rn(g, y[q][j], neu[j]);
-              upd[j] = __fmul_rn(g, x[j]);
-            }
-            row_update<DIM, P>(a, 1, tg[q], upd, y[q], slot_stream(key, q));
-          }
-          done = true;
-        }
-      }
-      if (!done) {
-#pragma unroll
-        for (int q = 0; q < NT; q++) {
-          if (tg[q] < 0) continue;
-          const float f = sg_dot<J>(x, y[q]);
-          const float g = sg_grad(f, q == 0 ? 1 : 0, s_exp, a.alpha);
-          float upd[J];
-#pragma unroll
-          for (int j = 0; j < J; j++) {
-            neu[j] = __fmaf_rn(g, y[q][j], neu[j]);
-            upd[j] = __fmul_rn(g, x[j]);
-          }
-          const bool stored = row_update<DIM, P>(a, 1, tg[q], upd, y[q], slot_stream(key, q));
-#pragma unroll
-          for (int r = q + 1; r < NT; r++)
-            if (tg[r] == tg[q])
-#pragma unroll
-              for (int j = 0; j < J; j++) y[r][j] = stored ? y[q][j] : __fadd_rn(y[q][j], upd[j]);
-        }
-      }
-      row_update<DIM, P>(a, 0, c_l1, neu, x, slot_stream(key, kSlotCtx));
-      my_pairs++;
-      pair++;
-      c_word = n_word;
-      c_l1 = n_l1;
-      c_t = n_t;
-      have = nhave;
-    }
-  }
-  if (lane == 0 && my_pairs) atomicAdd(a.pairs, my_pairs);
-}
-
 // cbow_kernel semantics (word2vec.cu:538-646, hs = 0) per warp: the mean of
 // the window's context rows (summed in window order, then divided by the
 // count) is scored against the positive and K negatives; every context row
