@@ -38,7 +38,7 @@
 extern "C" {
 #endif
 
-#define FELOG_ABI_VERSION 1
+#define FELOG_ABI_VERSION 2
 
 typedef enum felog_status {
   FELOG_OK = 0,
@@ -99,6 +99,8 @@ typedef struct felog_opts {
   uint64_t long_arena_tokens; /* spill arena for long walks (0: automatic) */
   uint64_t wait_limit;      /* spin limit of device-side waits (0: default) */
   int64_t hot_rows;         /* BF16 mode: FP32 master rows (0: the top 1% of the vocabulary, at least 1) */
+  float budget_confidence;  /* learned budget: predictions below this softmax confidence fall back (0: 0.9) */
+  float budget_audit;       /* learned budget: fraction of confident vertices re-checked (0: 0.05; <0: none) */
 } felog_opts;
 
 typedef struct felog_ctx felog_ctx;
@@ -241,6 +243,62 @@ felog_status felog_get_plan(felog_ctx *ctx, int32_t *sen, uint64_t *sent_start, 
 /* ---- budget ---- */
 felog_status felog_budget_check(felog_ctx *ctx, uint32_t round, felog_budget_stats *stats);
 felog_status felog_get_similarity(felog_ctx *ctx, float *sim);
+
+/* ---- learned walk budget (no reference counterpart) ----
+ * A 6 -> 64 -> 64 -> (9 + 1) MLP predicts each vertex's walk count (2..10)
+ * and walk length (20..80) from per-vertex features; in FELOG_BUDGET_LEARNED
+ * mode felog_budget_check lets confident predictions decide a vertex's stop
+ * flag without the convergence check, and runs the plain check (which
+ * decides) for the others and for an audited random sample. */
+#define FELOG_MLP_PARAMS 5258 /* W1[64][6] b1[64] W2[64][64] b2[64] W3[10][64] b3[10] */
+#define FELOG_MLP_STATE (FELOG_MLP_PARAMS + 12) /* + feature mean[6], 1/std[6] */
+#define FELOG_MLP_FEATURES 6
+
+typedef struct felog_mlp_opts {
+  int32_t epochs;     /* passes over the labelled vertices (0: 8) */
+  int32_t batch;      /* samples per Adam step, a multiple of 256 (0: 4096) */
+  float lr;           /* Adam step size (0: 3e-3) */
+  uint64_t seed;      /* initialisation and shuffling */
+} felog_mlp_opts;
+
+typedef struct felog_mlp_stats {
+  uint64_t samples;
+  uint64_t steps;
+  double loss_first;   /* mean loss of the first epoch */
+  double loss_last;    /* mean loss of the last epoch */
+  double count_accuracy; /* argmax count == label, over all samples */
+  double length_mae;   /* mean |predicted length - label| */
+  float ms;
+} felog_mlp_stats;
+
+/* Raw features of every vertex (V x 6 floats, host, optional):
+ * log1p(degree), log1p(weighted degree), entropy of the transition weights,
+ * log1p(2-hop degree sum), log1p(visits so far), log1p(first walk length).
+ * Needs at least one walk round. */
+felog_status felog_budget_features(felog_ctx *ctx, float *features);
+/* Labels recorded from the rounds run so far (plain criterion): count = the
+ * number of walks a vertex made until a convergence check stopped it (10 when
+ * none did), clipped to 2..10; length = its mean walk length, clipped to
+ * 20..80.  Host buffers of V entries, optional. */
+felog_status felog_budget_labels(felog_ctx *ctx, uint8_t *count, float *length);
+/* Trains the MLP on the GPU (own forward/backward/Adam kernels) on this
+ * context's features and recorded labels. */
+felog_status felog_mlp_train(felog_ctx *ctx, const felog_mlp_opts *opts, felog_mlp_stats *stats);
+/* Model state (FELOG_MLP_STATE floats: parameters, then the training graph's
+ * feature mean and 1/std, for information) to move a trained model between
+ * contexts.  Features are standardized with each graph's own moments, in
+ * training and in prediction. */
+felog_status felog_mlp_get_params(felog_ctx *ctx, float *state);
+felog_status felog_mlp_set_params(felog_ctx *ctx, const float *state);
+/* Mean loss gradient over n samples (host buffers; X standardized, n x 6),
+ * for checking the backward kernel: grad has FELOG_MLP_PARAMS floats. */
+felog_status felog_mlp_gradient(felog_ctx *ctx, const float *params, const float *X, const uint8_t *count,
+                                const float *length, uint64_t n, float *grad, double *loss);
+/* Inference for every vertex from its current features, standardized over
+ * this graph's walked vertices (needs a walk round and a model); outputs (V
+ * entries, host, optional) are also kept on the device for the learned budget
+ * check. */
+felog_status felog_mlp_predict(felog_ctx *ctx, uint8_t *count, float *confidence, float *length);
 
 /* ---- whole loop ---- */
 felog_status felog_run(felog_ctx *ctx, felog_run_stats *stats);

@@ -29,8 +29,22 @@ struct ConvArgs {
   float *sim;
   uint64_t seed;
   uint32_t round;
-  unsigned long long *counters;  // [evaluated, unconverged, stopped_total]
+  unsigned long long *counters;  // [evaluated, unconverged, stopped_total, predicted, audited, overruled,
+                                 //  audited_unconverged, evaluated_unconverged]
+  uint8_t *stop_round;           // round whose check stopped v (label recording)
+  // learned budget (pred_count == nullptr: plain criterion for every vertex)
+  const uint8_t *pred_count;
+  const float *pred_conf;
+  float conf_min;
+  uint32_t audit_threshold;      // audited when hash(seed, round, v) < this
 };
+
+// audit draw of vertex v in round r (uniform 32 bits)
+__device__ __forceinline__ uint32_t audit_hash(uint64_t seed, uint32_t round, uint32_t v) {
+  const uint4 o = philox4x32_10(make_uint4(v, round, 0x41554454u, 0u),
+                                make_uint2((uint32_t)seed ^ 0x9E3779B9u, (uint32_t)(seed >> 32)));
+  return o.x;
+}
 
 // First 30 positions of a partial Fisher-Yates shuffle of 0..deg-1 driven by
 // Philox (v, round, i); the same sequence as the oracle's orc_eval_choose.
@@ -79,10 +93,30 @@ __global__ void __launch_bounds__(256) k_converge(ConvArgs a) {
   const int wib = threadIdx.x >> 5;
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-  unsigned long long evaluated = 0, unconv = 0;
+  unsigned long long evaluated = 0, unconv = 0, predicted = 0, audited = 0, overruled = 0, aud_unconv = 0,
+                     eval_unconv = 0;
   for (uint32_t v = warp; v < a.v_num; v += nwarps) {
     // vertices outside the vocabulary (-min-count) have no row: not evaluated
     if (a.stop[v] || a.id2offset[v] == 0xFFFFFFFFu) continue;
+    // learned budget: a confident prediction decides unless v is audited
+    bool confident = false, learned_stop = false, audit = false;
+    if (a.pred_count) {
+      confident = a.pred_conf[v] >= a.conf_min;
+      learned_stop = a.round + 1 >= (uint32_t)a.pred_count[v];
+      audit = confident && audit_hash(a.seed, a.round, v) < a.audit_threshold;
+      if (confident && !audit) {
+        if (lane == 0) {
+          predicted++;
+          if (learned_stop) {
+            a.stop[v] = 1;
+            if (a.stop_round) a.stop_round[v] = (uint8_t)min(a.round, 254u);
+          } else {
+            unconv++;
+          }
+        }
+        continue;
+      }
+    }
     evaluated++;
     const uint64_t b = a.row_ptr[v];
     const uint32_t deg = (uint32_t)(a.row_ptr[v + 1] - b);
@@ -121,13 +155,29 @@ __global__ void __launch_bounds__(256) k_converge(ConvArgs a) {
     const float s = used > 0 ? __fdiv_rn(sum, (float)used) : 0.0f;
     if (lane == 0) {
       a.sim[v] = s;
-      if ((double)s > 0.65) a.stop[v] = 1;
-      else unconv++;
+      const bool plain_stop = (double)s > 0.65;
+      if (plain_stop) {
+        a.stop[v] = 1;
+        if (a.stop_round) a.stop_round[v] = (uint8_t)min(a.round, 254u);
+      } else {
+        unconv++;
+        eval_unconv++;
+      }
+      if (audit) {
+        audited++;
+        overruled += plain_stop != learned_stop;
+        aud_unconv += !plain_stop;
+      }
     }
   }
   if (lane == 0) {
     if (evaluated) atomicAdd(&a.counters[0], evaluated);
     if (unconv) atomicAdd(&a.counters[1], unconv);
+    if (predicted) atomicAdd(&a.counters[3], predicted);
+    if (audited) atomicAdd(&a.counters[4], audited);
+    if (overruled) atomicAdd(&a.counters[5], overruled);
+    if (aud_unconv) atomicAdd(&a.counters[6], aud_unconv);
+    if (eval_unconv) atomicAdd(&a.counters[7], eval_unconv);
   }
 }
 

@@ -13,12 +13,14 @@
 #include <cstring>
 #include <new>
 #include <numeric>
+#include <random>
 #include <string>
 #include <vector>
 
 #include "budget.cuh"
 #include "common.cuh"
 #include "graph.cuh"
+#include "mlp.cuh"
 #include "pairs.cuh"
 #include "plan.cuh"
 #include "sgns.cuh"
@@ -130,6 +132,15 @@ struct felog_ctx {
 
   // budget
   DevBuf<float> sim;
+  // learned budget: per-vertex records of the rounds run (labels, features)
+  DevBuf<uint32_t> bud_walks, bud_len_sum, bud_first_len;
+  DevBuf<uint8_t> bud_stop_round;
+  DevBuf<float> feat, mlp_params, mlp_m1, mlp_m2, mlp_partial, mlp_norm, mlp_grad, pred_conf, pred_len;
+  DevBuf<double> mlp_loss;
+  DevBuf<uint32_t> mlp_idx;
+  DevBuf<uint8_t> mlp_ycount, pred_count;
+  DevBuf<float> mlp_ylen;
+  bool mlp_ready = false, pred_ready = false;
   uint64_t last_eva = 0;
   bool have_last_eva = false;
 
@@ -278,7 +289,7 @@ extern "C" void felog_destroy(felog_ctx *c) {
   c->exp_table.release(); c->syn0.release(); c->syn1.release(); c->syn0_bf.release(); c->syn1_bf.release(); c->jump.release();
   c->p_cand.release(); c->p_draws.release(); c->p_cons.release(); c->p_kept.release(); c->p_blk.release();
   c->p_state.release(); c->p_neg_state.release(); c->p_out_off.release(); c->p_batch_first.release();
-  c->p_sen.release(); c->pr_count.release(); c->pr_off.release(); c->pr_rec.release(); c->pr_cstate.release(); c->pr_jump.release(); c->pr_cfirst.release(); c->p_negs.release(); c->sim.release(); c->cub_tmp.release(); c->out_tmp.release();
+  c->p_sen.release(); c->pr_count.release(); c->pr_off.release(); c->pr_rec.release(); c->pr_cstate.release(); c->pr_jump.release(); c->pr_cfirst.release(); c->p_negs.release(); c->sim.release(); c->bud_walks.release(); c->bud_len_sum.release(); c->bud_first_len.release(); c->bud_stop_round.release(); c->feat.release(); c->mlp_params.release(); c->mlp_m1.release(); c->mlp_m2.release(); c->mlp_partial.release(); c->mlp_norm.release(); c->mlp_grad.release(); c->pred_conf.release(); c->pred_len.release(); c->mlp_loss.release(); c->mlp_idx.release(); c->mlp_ycount.release(); c->pred_count.release(); c->mlp_ylen.release(); c->cub_tmp.release(); c->out_tmp.release();
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
   if (c->tm0) cudaEventDestroy(c->tm0);
@@ -493,6 +504,31 @@ felog_status build_active(felog_ctx *c, uint32_t walker_num) {
   return FELOG_OK;
 }
 
+// per start vertex: walks, their total length, the first walk's length
+__global__ void k_budget_record_walk(const uint32_t *active, uint32_t n_active, uint32_t v_num,
+                                     const uint32_t *sent_len, uint32_t *walks, uint32_t *len_sum,
+                                     uint32_t *first_len) {
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n_active; k += gridDim.x * blockDim.x) {
+    const uint32_t v = active[k] % v_num;
+    const uint32_t old = atomicAdd(&walks[v], 1u);
+    atomicAdd(&len_sum[v], sent_len[k]);
+    if (old == 0) first_len[v] = sent_len[k];
+  }
+}
+
+felog_status budget_records(felog_ctx *c) {
+  if (c->bud_walks.p && c->bud_walks.n >= c->V) return FELOG_OK;
+  CK(c->bud_walks.ensure(c->V), "budget records");
+  CK(c->bud_len_sum.ensure(c->V), "budget records");
+  CK(c->bud_first_len.ensure(c->V), "budget records");
+  CK(c->bud_stop_round.ensure(c->V), "budget records");
+  CK(cudaMemsetAsync(c->bud_walks.p, 0, 4 * (size_t)c->V, c->stream), "budget records");
+  CK(cudaMemsetAsync(c->bud_len_sum.p, 0, 4 * (size_t)c->V, c->stream), "budget records");
+  CK(cudaMemsetAsync(c->bud_first_len.p, 0, 4 * (size_t)c->V, c->stream), "budget records");
+  CK(cudaMemsetAsync(c->bud_stop_round.p, 0xFF, (size_t)c->V, c->stream), "budget records");
+  return FELOG_OK;
+}
+
 felog_status round_kl(felog_ctx *c, double *out) {
   const int nb = 256;
   CK(c->kl_partial.ensure(nb + 1), "kl");
@@ -606,6 +642,15 @@ extern "C" felog_status felog_walk_round(felog_ctx *c, uint32_t round, const fel
   c->n_sent = na;
   c->n_tok = h[0];
   c->corpus_ready = true;
+  s = budget_records(c);
+  if (s != FELOG_OK) return s;
+  if (na) {
+    k_budget_record_walk<<<grid_for(c, na, 256), 256, 0, c->stream>>>(c->active.p, na, c->V, c->sent_len.p,
+                                                                     c->bud_walks.p, c->bud_len_sum.p,
+                                                                     c->bud_first_len.p);
+    c->launches++;
+    CK(cudaGetLastError(), "walk_round: budget records");
+  }
   c->words_sum_cum += h[0];
   if (stats) {
     memset(stats, 0, sizeof(*stats));
@@ -1328,8 +1373,21 @@ extern "C" felog_status felog_budget_check(felog_ctx *c, uint32_t round, felog_b
   if (!c) return FELOG_INVALID_ARG;
   if (!c->model_ready) return fail(c, FELOG_NOT_READY, "model not initialised");
   CK(cudaSetDevice(c->device), "budget_check");
-  CK(cudaMemsetAsync(c->counters.p, 0, sizeof(unsigned long long) * 4, c->stream), "budget_check");
+  CK(cudaMemsetAsync(c->counters.p, 0, sizeof(unsigned long long) * 8, c->stream), "budget_check");
+  const bool learned = c->o.budget_mode == FELOG_BUDGET_LEARNED;
+  if (learned && !c->pred_ready)
+    return fail(c, FELOG_NOT_READY, "learned budget: no predictions (felog_mlp_predict after a walk round)");
+  felog_status bs0 = budget_records(c);
+  if (bs0 != FELOG_OK) return bs0;
   ConvArgs a{};
+  a.stop_round = c->bud_stop_round.p;
+  if (learned) {
+    a.pred_count = c->pred_count.p;
+    a.pred_conf = c->pred_conf.p;
+    a.conf_min = c->o.budget_confidence > 0.0f ? c->o.budget_confidence : 0.9f;
+    const double audit = c->o.budget_audit == 0.0f ? 0.05 : std::max(0.0, (double)c->o.budget_audit);
+    a.audit_threshold = (uint32_t)std::min(4294967295.0, audit * 4294967296.0);
+  }
   a.rows.syn0 = c->syn0.p;
   a.rows.syn0_bf = c->syn0_bf.p;
   a.rows.n_hot = c->n_f32;
@@ -1362,16 +1420,24 @@ extern "C" felog_status felog_budget_check(felog_ctx *c, uint32_t round, felog_b
   c->launches++;
   CK(cudaGetLastError(), "budget_check");
   CK(cudaEventRecord(c->ev1, c->stream), "budget_check");
-  unsigned long long h[4];
+  unsigned long long h[8];
   CK(cudaMemcpyAsync(h, c->counters.p, sizeof h, cudaMemcpyDeviceToHost, c->stream), "budget_check");
   CK(cudaStreamSynchronize(c->stream), "budget_check");
   float ms = 0;
   CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1), "budget_check");
-  // eva_num ratio test (word2vec.cu:2073-2080); the first comparison is against vocab_size
+  // eva_num ratio test (word2vec.cu:2073-2080); the first comparison is against
+  // vocab_size.  Learned mode: the plain criterion's count among the confident
+  // (predicted or audited) vertices is estimated from the audited random
+  // sample, so that the test follows what the plain criterion would decide.
+  uint64_t eva = h[1];
+  if (learned && h[4] > 0) {
+    const double conf_unconv = (double)h[6] / (double)h[4] * (double)(h[3] + h[4]);
+    eva = (uint64_t)std::llround((double)(h[7] - h[6]) + conf_unconv);
+  }
   uint64_t last = c->have_last_eva ? c->last_eva : (uint64_t)c->vocab_size;
-  float ratio = last ? (float)h[1] / (float)last : 0.0f;
+  float ratio = last ? (float)eva / (float)last : 0.0f;
   int stop_all = (last != 0 && ratio > 0.7f) ? 1 : 0;
-  c->last_eva = h[1];
+  c->last_eva = eva;
   c->have_last_eva = true;
   if (stats) {
     memset(stats, 0, sizeof(*stats));
@@ -1379,6 +1445,9 @@ extern "C" felog_status felog_budget_check(felog_ctx *c, uint32_t round, felog_b
     stats->unconverged = h[1];
     stats->stopped_total = h[2];
     stats->stop_all = stop_all;
+    stats->predicted = h[3];
+    stats->audited = h[4];
+    stats->overruled = h[5];
     stats->ms = ms;
   }
   return FELOG_OK;
@@ -1388,6 +1457,356 @@ extern "C" felog_status felog_get_similarity(felog_ctx *c, float *sim) {
   if (!c || !sim) return FELOG_INVALID_ARG;
   if (!c->model_ready) return fail(c, FELOG_NOT_READY, "model not initialised");
   CK(cudaMemcpy(sim, c->sim.p, 4 * (size_t)c->V, cudaMemcpyDeviceToHost), "get_similarity");
+  return FELOG_OK;
+}
+
+// -------------------------------------------------------- learned budget
+
+namespace {
+
+felog_status compute_features(felog_ctx *c) {
+  if (!c->V) return fail(c, FELOG_NOT_READY, "no graph loaded");
+  if (!c->bud_walks.p || !c->visit_freq.p) return fail(c, FELOG_NOT_READY, "budget features need a walk round");
+  CK(c->feat.ensure((size_t)c->V * kMlpIn), "budget features");
+  k_budget_features<<<grid_for(c, (uint64_t)c->V * 32, 256), 256, 0, c->stream>>>(
+      c->row_ptr.p, c->adj.p, c->V, c->visit_freq.p, c->bud_first_len.p, c->feat.p);
+  c->launches++;
+  CK(cudaGetLastError(), "budget features");
+  return FELOG_OK;
+}
+
+felog_status host_labels(felog_ctx *c, std::vector<uint8_t> &cnt, std::vector<float> &len,
+                         std::vector<uint32_t> &walks) {
+  if (!c->bud_walks.p) return fail(c, FELOG_NOT_READY, "no rounds recorded");
+  const uint32_t V = c->V;
+  std::vector<uint8_t> sr(V);
+  std::vector<uint32_t> ls(V);
+  walks.resize(V);
+  CK(cudaStreamSynchronize(c->stream), "budget labels");
+  CK(cudaMemcpy(sr.data(), c->bud_stop_round.p, V, cudaMemcpyDeviceToHost), "budget labels");
+  CK(cudaMemcpy(ls.data(), c->bud_len_sum.p, 4 * (size_t)V, cudaMemcpyDeviceToHost), "budget labels");
+  CK(cudaMemcpy(walks.data(), c->bud_walks.p, 4 * (size_t)V, cudaMemcpyDeviceToHost), "budget labels");
+  cnt.resize(V);
+  len.resize(V);
+  for (uint32_t v = 0; v < V; v++) {
+    const int k = sr[v] == 0xFF ? 10 : (int)sr[v] + 1;
+    cnt[v] = (uint8_t)std::min(10, std::max(2, k));
+    const float l = walks[v] ? (float)ls[v] / (float)walks[v] : 20.0f;
+    len[v] = std::min(80.0f, std::max(20.0f, l));
+  }
+  return FELOG_OK;
+}
+
+// mean and 1/std of each raw feature over the vertices that have walked (FP64)
+felog_status graph_feature_norm(felog_ctx *c, float *norm, std::vector<uint32_t> *walked) {
+  const uint32_t V = c->V;
+  std::vector<float> fh((size_t)V * kMlpIn);
+  std::vector<uint32_t> walks(V);
+  CK(cudaStreamSynchronize(c->stream), "feature norm");
+  CK(cudaMemcpy(fh.data(), c->feat.p, 4 * fh.size(), cudaMemcpyDeviceToHost), "feature norm");
+  CK(cudaMemcpy(walks.data(), c->bud_walks.p, 4 * (size_t)V, cudaMemcpyDeviceToHost), "feature norm");
+  std::vector<uint32_t> idx;
+  for (uint32_t v = 0; v < V; v++)
+    if (walks[v]) idx.push_back(v);
+  if (idx.empty()) return fail(c, FELOG_NOT_READY, "no vertex has walked");
+  for (int k = 0; k < kMlpIn; k++) {
+    double m = 0, q = 0;
+    for (uint32_t v : idx) m += fh[(size_t)v * kMlpIn + k];
+    m /= idx.size();
+    for (uint32_t v : idx) q += (fh[(size_t)v * kMlpIn + k] - m) * (fh[(size_t)v * kMlpIn + k] - m);
+    const double sd = std::sqrt(q / idx.size());
+    norm[k] = (float)m;
+    norm[kMlpIn + k] = sd > 1e-12 ? (float)(1.0 / sd) : 1.0f;
+  }
+  if (walked) *walked = std::move(idx);
+  return FELOG_OK;
+}
+
+felog_status mlp_buffers(felog_ctx *c) {
+  CK(c->mlp_params.ensure(kMlpParams), "mlp");
+  CK(c->mlp_norm.ensure(2 * kMlpIn), "mlp");
+  CK(c->mlp_m1.ensure(kMlpParams), "mlp");
+  CK(c->mlp_m2.ensure(kMlpParams), "mlp");
+  CK(c->mlp_grad.ensure(kMlpParams), "mlp");
+  static bool attr_set[64] = {false};
+  if (c->device < 64 && !attr_set[c->device]) {
+    CK(cudaFuncSetAttribute(k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)(sizeof(float) * (kMlpParams + kMlpBatch * (2 * kMlpPad + kMlpOut + kMlpIn)))),
+       "mlp");
+    attr_set[c->device] = true;
+  }
+  return FELOG_OK;
+}
+
+constexpr size_t kMlpSmem = sizeof(float) * (kMlpParams + kMlpBatch * (2 * kMlpPad + kMlpOut + kMlpIn));
+
+}  // namespace
+
+extern "C" felog_status felog_budget_features(felog_ctx *c, float *features) {
+  if (!c) return FELOG_INVALID_ARG;
+  CK(cudaSetDevice(c->device), "budget features");
+  felog_status s = compute_features(c);
+  if (s != FELOG_OK) return s;
+  if (features)
+    CK(cudaMemcpyAsync(features, c->feat.p, 4 * (size_t)c->V * kMlpIn, cudaMemcpyDeviceToHost, c->stream),
+       "budget features");
+  CK(cudaStreamSynchronize(c->stream), "budget features");
+  return FELOG_OK;
+}
+
+extern "C" felog_status felog_budget_labels(felog_ctx *c, uint8_t *count, float *length) {
+  if (!c) return FELOG_INVALID_ARG;
+  std::vector<uint8_t> cnt;
+  std::vector<float> len;
+  std::vector<uint32_t> walks;
+  felog_status s = host_labels(c, cnt, len, walks);
+  if (s != FELOG_OK) return s;
+  if (count) memcpy(count, cnt.data(), cnt.size());
+  if (length) memcpy(length, len.data(), 4 * len.size());
+  return FELOG_OK;
+}
+
+extern "C" felog_status felog_mlp_train(felog_ctx *c, const felog_mlp_opts *opts, felog_mlp_stats *stats) {
+  if (!c) return FELOG_INVALID_ARG;
+  felog_mlp_opts o{};
+  if (opts) o = *opts;
+  if (o.epochs <= 0) o.epochs = 8;
+  if (o.batch <= 0) o.batch = 4096;
+  if (o.batch % kMlpBatch) return fail(c, FELOG_INVALID_ARG, "mlp batch must be a multiple of %d", kMlpBatch);
+  if (o.lr <= 0.0f) o.lr = 3e-3f;
+  CK(cudaSetDevice(c->device), "mlp_train");
+  CK(cudaEventRecord(c->ev0, c->stream), "mlp_train");
+  felog_status s = compute_features(c);
+  if (s != FELOG_OK) return s;
+  s = mlp_buffers(c);
+  if (s != FELOG_OK) return s;
+  std::vector<uint8_t> cnt;
+  std::vector<float> len;
+  std::vector<uint32_t> walks;
+  s = host_labels(c, cnt, len, walks);
+  if (s != FELOG_OK) return s;
+  const uint32_t V = c->V;
+  // features standardized over this graph's walked vertices (FP64 moments)
+  std::vector<uint32_t> idx;
+  float norm[2 * kMlpIn];
+  s = graph_feature_norm(c, norm, &idx);
+  if (s != FELOG_OK) return s;
+  CK(cudaMemcpy(c->mlp_norm.p, norm, sizeof norm, cudaMemcpyHostToDevice), "mlp_train");
+  k_budget_standardize<<<grid_for(c, (uint64_t)V * kMlpIn, 256), 256, 0, c->stream>>>(c->feat.p, V, c->mlp_norm.p,
+                                                                                      c->mlp_norm.p + kMlpIn);
+  c->launches++;
+  CK(c->mlp_ycount.ensure(V), "mlp_train");
+  CK(c->mlp_ylen.ensure(V), "mlp_train");
+  CK(cudaMemcpy(c->mlp_ycount.p, cnt.data(), V, cudaMemcpyHostToDevice), "mlp_train");
+  CK(cudaMemcpy(c->mlp_ylen.p, len.data(), 4 * (size_t)V, cudaMemcpyHostToDevice), "mlp_train");
+  // He-uniform initialisation, zero biases
+  std::mt19937_64 rng(o.seed ^ 0x4D4C5031ULL);
+  std::vector<float> P(kMlpParams, 0.0f);
+  auto fill = [&](int off, int n, int fan_in) {
+    const float r = std::sqrt(6.0f / (float)fan_in);
+    std::uniform_real_distribution<float> U(-r, r);
+    for (int i = 0; i < n; i++) P[off + i] = U(rng);
+  };
+  fill(kMlpW1, kMlpH * kMlpIn, kMlpIn);
+  fill(kMlpW2, kMlpH * kMlpH, kMlpH);
+  fill(kMlpW3, kMlpOut * kMlpH, kMlpH);
+  CK(cudaMemcpy(c->mlp_params.p, P.data(), 4 * P.size(), cudaMemcpyHostToDevice), "mlp_train");
+  CK(cudaMemset(c->mlp_m1.p, 0, 4 * kMlpParams), "mlp_train");
+  CK(cudaMemset(c->mlp_m2.p, 0, 4 * kMlpParams), "mlp_train");
+  const uint64_t n = idx.size();
+  const int max_blocks = o.batch / kMlpBatch;
+  CK(c->mlp_partial.ensure((size_t)max_blocks * kMlpParams), "mlp_train");
+  CK(c->mlp_idx.ensure(n), "mlp_train");
+  CK(c->mlp_loss.ensure(n / kMlpBatch + 2), "mlp_train");
+  std::vector<double> lp(n / kMlpBatch + 2);
+  uint64_t steps = 0;
+  double loss_first = 0, loss_last = 0;
+  const float b1 = 0.9f, b2 = 0.999f;
+  for (int ep = 0; ep < o.epochs; ep++) {
+    std::shuffle(idx.begin(), idx.end(), rng);
+    CK(cudaMemcpyAsync(c->mlp_idx.p, idx.data(), 4 * n, cudaMemcpyHostToDevice, c->stream), "mlp_train");
+    uint64_t nblk_total = 0;
+    for (uint64_t b0 = 0; b0 < n; b0 += o.batch) {
+      const uint64_t nb = std::min<uint64_t>(o.batch, n - b0);
+      const int blocks = (int)((nb + kMlpBatch - 1) / kMlpBatch);
+      MlpGradArgs ga{};
+      ga.params = c->mlp_params.p;
+      ga.X = c->feat.p;
+      ga.y_count = c->mlp_ycount.p;
+      ga.y_len = c->mlp_ylen.p;
+      ga.idx = c->mlp_idx.p + b0;
+      ga.n = nb;
+      ga.partial = c->mlp_partial.p;
+      ga.loss_partial = c->mlp_loss.p + nblk_total;
+      k_mlp_grad<<<blocks, kMlpBatch, kMlpSmem, c->stream>>>(ga);
+      c->launches++;
+      steps++;
+      const float bc1 = 1.0f - std::pow(b1, (float)steps), bc2 = 1.0f - std::pow(b2, (float)steps);
+      k_mlp_adam<<<(kMlpParams + 255) / 256, 256, 0, c->stream>>>(c->mlp_params.p, c->mlp_m1.p, c->mlp_m2.p,
+                                                                  c->mlp_partial.p, blocks, 1.0f / (float)nb, o.lr,
+                                                                  b1, b2, 1e-8f, bc1, bc2, nullptr);
+      c->launches++;
+      nblk_total += blocks;
+    }
+    CK(cudaGetLastError(), "mlp_train");
+    CK(cudaMemcpyAsync(lp.data(), c->mlp_loss.p, 8 * nblk_total, cudaMemcpyDeviceToHost, c->stream), "mlp_train");
+    CK(cudaStreamSynchronize(c->stream), "mlp_train");
+    double l = 0;
+    for (uint64_t i = 0; i < nblk_total; i++) l += lp[i];
+    l /= (double)n;
+    if (ep == 0) loss_first = l;
+    loss_last = l;
+  }
+  c->mlp_ready = true;
+  // fit on the training vertices
+  CK(c->pred_count.ensure(V), "mlp_train");
+  CK(c->pred_conf.ensure(V), "mlp_train");
+  CK(c->pred_len.ensure(V), "mlp_train");
+  k_mlp_infer<<<grid_for(c, V, 128), 128, 0, c->stream>>>(c->mlp_params.p, c->feat.p, V, c->pred_count.p,
+                                                          c->pred_conf.p, c->pred_len.p);
+  c->launches++;
+  CK(cudaGetLastError(), "mlp_train");
+  CK(cudaEventRecord(c->ev1, c->stream), "mlp_train");
+  std::vector<uint8_t> pc(V);
+  std::vector<float> pl(V);
+  CK(cudaMemcpyAsync(pc.data(), c->pred_count.p, V, cudaMemcpyDeviceToHost, c->stream), "mlp_train");
+  CK(cudaMemcpyAsync(pl.data(), c->pred_len.p, 4 * (size_t)V, cudaMemcpyDeviceToHost, c->stream), "mlp_train");
+  CK(cudaStreamSynchronize(c->stream), "mlp_train");
+  c->pred_ready = false;  // predictions for the budget check come from felog_mlp_predict
+  if (stats) {
+    memset(stats, 0, sizeof(*stats));
+    uint64_t ok = 0;
+    double mae = 0;
+    for (uint32_t v : idx) {
+      ok += pc[v] == cnt[v];
+      mae += std::fabs((double)pl[v] - (double)len[v]);
+    }
+    stats->samples = n;
+    stats->steps = steps;
+    stats->loss_first = loss_first;
+    stats->loss_last = loss_last;
+    stats->count_accuracy = (double)ok / (double)n;
+    stats->length_mae = mae / (double)n;
+    CK(cudaEventElapsedTime(&stats->ms, c->ev0, c->ev1), "mlp_train");
+  }
+  return FELOG_OK;
+}
+
+extern "C" felog_status felog_mlp_get_params(felog_ctx *c, float *state) {
+  if (!c || !state) return FELOG_INVALID_ARG;
+  if (!c->mlp_ready) return fail(c, FELOG_NOT_READY, "no trained model");
+  CK(cudaMemcpy(state, c->mlp_params.p, 4 * kMlpParams, cudaMemcpyDeviceToHost), "mlp_get_params");
+  CK(cudaMemcpy(state + kMlpParams, c->mlp_norm.p, 4 * 2 * kMlpIn, cudaMemcpyDeviceToHost), "mlp_get_params");
+  return FELOG_OK;
+}
+
+extern "C" felog_status felog_mlp_set_params(felog_ctx *c, const float *state) {
+  if (!c || !state) return FELOG_INVALID_ARG;
+  CK(cudaSetDevice(c->device), "mlp_set_params");
+  felog_status s = mlp_buffers(c);
+  if (s != FELOG_OK) return s;
+  CK(cudaMemcpy(c->mlp_params.p, state, 4 * kMlpParams, cudaMemcpyHostToDevice), "mlp_set_params");
+  CK(cudaMemcpy(c->mlp_norm.p, state + kMlpParams, 4 * 2 * kMlpIn, cudaMemcpyHostToDevice), "mlp_set_params");
+  c->mlp_ready = true;
+  c->pred_ready = false;
+  return FELOG_OK;
+}
+
+extern "C" felog_status felog_mlp_gradient(felog_ctx *c, const float *params, const float *X, const uint8_t *count,
+                                          const float *length, uint64_t n, float *grad, double *loss) {
+  if (!c || !params || !X || !count || !length || !grad || n == 0) return FELOG_INVALID_ARG;
+  for (uint64_t i = 0; i < n; i++)
+    if (count[i] < 2 || count[i] > 10) return fail(c, FELOG_INVALID_ARG, "mlp_gradient: count label outside 2..10");
+  CK(cudaSetDevice(c->device), "mlp_gradient");
+  felog_status s = mlp_buffers(c);
+  if (s != FELOG_OK) return s;
+  const int blocks = (int)((n + kMlpBatch - 1) / kMlpBatch);
+  float *dP = nullptr, *dX = nullptr, *dL = nullptr, *dPart = nullptr, *dG = nullptr;
+  uint8_t *dC = nullptr;
+  uint32_t *dI = nullptr;
+  double *dLoss = nullptr;
+  cudaError_t e = cudaMalloc(&dP, 4 * kMlpParams);
+  if (e == cudaSuccess) e = cudaMalloc(&dX, 4 * n * kMlpIn);
+  if (e == cudaSuccess) e = cudaMalloc(&dL, 4 * n);
+  if (e == cudaSuccess) e = cudaMalloc(&dC, n);
+  if (e == cudaSuccess) e = cudaMalloc(&dI, 4 * n);
+  if (e == cudaSuccess) e = cudaMalloc(&dPart, 4 * (size_t)blocks * kMlpParams);
+  if (e == cudaSuccess) e = cudaMalloc(&dG, 4 * kMlpParams);
+  if (e == cudaSuccess) e = cudaMalloc(&dLoss, 8 * (size_t)blocks);
+  std::vector<uint32_t> id(n);
+  std::iota(id.begin(), id.end(), 0u);
+  if (e == cudaSuccess) e = cudaMemcpy(dP, params, 4 * kMlpParams, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(dX, X, 4 * n * kMlpIn, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(dL, length, 4 * n, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(dC, count, n, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(dI, id.data(), 4 * n, cudaMemcpyHostToDevice);
+  std::vector<double> lp(blocks);
+  if (e == cudaSuccess) {
+    MlpGradArgs ga{};
+    ga.params = dP;
+    ga.X = dX;
+    ga.y_count = dC;
+    ga.y_len = dL;
+    ga.idx = dI;
+    ga.n = n;
+    ga.partial = dPart;
+    ga.loss_partial = dLoss;
+    k_mlp_grad<<<blocks, kMlpBatch, kMlpSmem, c->stream>>>(ga);
+    c->launches++;
+    k_mlp_adam<<<(kMlpParams + 255) / 256, 256, 0, c->stream>>>(dP, nullptr, nullptr, dPart, blocks, 1.0f / (float)n,
+                                                                0.0f, 0.f, 0.f, 0.f, 1.f, 1.f, dG);
+    c->launches++;
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e == cudaSuccess) e = cudaMemcpy(grad, dG, 4 * kMlpParams, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(lp.data(), dLoss, 8 * (size_t)blocks, cudaMemcpyDeviceToHost);
+  }
+  cudaFree(dP);
+  cudaFree(dX);
+  cudaFree(dL);
+  cudaFree(dC);
+  cudaFree(dI);
+  cudaFree(dPart);
+  cudaFree(dG);
+  cudaFree(dLoss);
+  if (e != cudaSuccess) return cuda_fail(c, e, "mlp_gradient");
+  if (loss) {
+    double l = 0;
+    for (double x : lp) l += x;
+    *loss = l / (double)n;
+  }
+  return FELOG_OK;
+}
+
+extern "C" felog_status felog_mlp_predict(felog_ctx *c, uint8_t *count, float *confidence, float *length) {
+  if (!c) return FELOG_INVALID_ARG;
+  if (!c->mlp_ready) return fail(c, FELOG_NOT_READY, "no trained model (felog_mlp_train or felog_mlp_set_params)");
+  CK(cudaSetDevice(c->device), "mlp_predict");
+  felog_status s = compute_features(c);
+  if (s != FELOG_OK) return s;
+  const uint32_t V = c->V;
+  // standardize with this graph's own feature moments, as in training
+  float norm[2 * kMlpIn];
+  s = graph_feature_norm(c, norm, nullptr);
+  if (s != FELOG_OK) return s;
+  CK(c->mlp_grad.ensure(kMlpParams), "mlp_predict");
+  CK(cudaMemcpyAsync(c->mlp_grad.p, norm, sizeof norm, cudaMemcpyHostToDevice, c->stream), "mlp_predict");
+  k_budget_standardize<<<grid_for(c, (uint64_t)V * kMlpIn, 256), 256, 0, c->stream>>>(c->feat.p, V, c->mlp_grad.p,
+                                                                                      c->mlp_grad.p + kMlpIn);
+  c->launches++;
+  CK(c->pred_count.ensure(V), "mlp_predict");
+  CK(c->pred_conf.ensure(V), "mlp_predict");
+  CK(c->pred_len.ensure(V), "mlp_predict");
+  k_mlp_infer<<<grid_for(c, V, 128), 128, 0, c->stream>>>(c->mlp_params.p, c->feat.p, V, c->pred_count.p,
+                                                          c->pred_conf.p, c->pred_len.p);
+  c->launches++;
+  CK(cudaGetLastError(), "mlp_predict");
+  if (count) CK(cudaMemcpyAsync(count, c->pred_count.p, V, cudaMemcpyDeviceToHost, c->stream), "mlp_predict");
+  if (confidence)
+    CK(cudaMemcpyAsync(confidence, c->pred_conf.p, 4 * (size_t)V, cudaMemcpyDeviceToHost, c->stream), "mlp_predict");
+  if (length) CK(cudaMemcpyAsync(length, c->pred_len.p, 4 * (size_t)V, cudaMemcpyDeviceToHost, c->stream), "mlp_predict");
+  CK(cudaStreamSynchronize(c->stream), "mlp_predict");
+  c->pred_ready = true;
   return FELOG_OK;
 }
 
@@ -1408,6 +1827,10 @@ extern "C" felog_status felog_run(felog_ctx *c, felog_run_stats *st) {
     felog_walk_stats ws;
     s = felog_walk_round(c, r, nullptr, &ws);
     if (s != FELOG_OK) return s;
+    if (c->o.budget_mode == FELOG_BUDGET_LEARNED && !c->pred_ready) {
+      s = felog_mlp_predict(c, nullptr, nullptr, nullptr);  // features from the first round's walks
+      if (s != FELOG_OK) return s;
+    }
     felog_train_stats ts;
     s = felog_train_round(c, r, -1.0f, &ts);
     if (s != FELOG_OK) return s;

@@ -43,7 +43,7 @@ class FelogOpts(ctypes.Structure):
         ("weighted", ctypes.c_int32), ("budget_mode", ctypes.c_int32), ("max_rounds", ctypes.c_int32),
         ("device", ctypes.c_int32), ("slot_len", ctypes.c_int32), ("seed", ctypes.c_uint64),
         ("long_arena_tokens", ctypes.c_uint64), ("wait_limit", ctypes.c_uint64),
-        ("hot_rows", ctypes.c_int64),
+        ("hot_rows", ctypes.c_int64), ("budget_confidence", ctypes.c_float), ("budget_audit", ctypes.c_float),
     ]
 
 
@@ -70,6 +70,21 @@ class BudgetStats(ctypes.Structure):
     _fields_ = [("evaluated", ctypes.c_uint64), ("unconverged", ctypes.c_uint64),
                 ("stopped_total", ctypes.c_uint64), ("predicted", ctypes.c_uint64), ("audited", ctypes.c_uint64),
                 ("overruled", ctypes.c_uint64), ("stop_all", ctypes.c_int32), ("ms", ctypes.c_float)]
+
+
+class MlpOpts(ctypes.Structure):
+    _fields_ = [("epochs", ctypes.c_int32), ("batch", ctypes.c_int32), ("lr", ctypes.c_float),
+                ("seed", ctypes.c_uint64)]
+
+
+class MlpStats(ctypes.Structure):
+    _fields_ = [("samples", ctypes.c_uint64), ("steps", ctypes.c_uint64), ("loss_first", ctypes.c_double),
+                ("loss_last", ctypes.c_double), ("count_accuracy", ctypes.c_double), ("length_mae", ctypes.c_double),
+                ("ms", ctypes.c_float)]
+
+
+MLP_PARAMS = 5258
+MLP_STATE = MLP_PARAMS + 12
 
 
 class RunStats(ctypes.Structure):
@@ -132,6 +147,13 @@ def gpu_lib():
         L.felog_set_embeddings.argtypes = [_P, _P, _P]
         L.felog_plan_size.argtypes = [_P, _P, _P, _P]
         L.felog_score_pairs.argtypes = [_P, _P, _P, _P, _P, ctypes.c_uint64, ctypes.c_uint64, _P, _P]
+        L.felog_budget_features.argtypes = [_P, _P]
+        L.felog_budget_labels.argtypes = [_P, _P, _P]
+        L.felog_mlp_train.argtypes = [_P, ctypes.POINTER(MlpOpts), ctypes.POINTER(MlpStats)]
+        L.felog_mlp_get_params.argtypes = [_P, _P]
+        L.felog_mlp_set_params.argtypes = [_P, _P]
+        L.felog_mlp_gradient.argtypes = [_P, _P, _P, _P, _P, ctypes.c_uint64, _P, ctypes.POINTER(ctypes.c_double)]
+        L.felog_mlp_predict.argtypes = [_P, _P, _P, _P]
         L.felog_get_plan.argtypes = [_P, _P, _P, _P, _P]
         L.felog_budget_check.argtypes = [_P, ctypes.c_uint32, ctypes.POINTER(BudgetStats)]
         L.felog_get_similarity.argtypes = [_P, _P]
@@ -343,6 +365,53 @@ class Felog:
         self._ck(self._L.felog_score_pairs(self.h, _addr(c), _addr(t), _addr(lab), _addr(b), len(c), n_batches,
                                            _addr(dots), _addr(loss)))
         return dots[: len(c)], loss[:n_batches]
+
+    # ---- learned walk budget
+    def budget_features(self):
+        f = np.zeros(self.opts.v_num * 6, np.float32)
+        self._ck(self._L.felog_budget_features(self.h, _addr(f)))
+        return f.reshape(-1, 6)
+
+    def budget_labels(self):
+        c = np.zeros(self.opts.v_num, np.uint8)
+        l = np.zeros(self.opts.v_num, np.float32)
+        self._ck(self._L.felog_budget_labels(self.h, _addr(c), _addr(l)))
+        return c, l
+
+    def mlp_train(self, epochs=0, batch=0, lr=0.0, seed=1):
+        o = MlpOpts(epochs, batch, lr, seed)
+        st = MlpStats()
+        self._ck(self._L.felog_mlp_train(self.h, ctypes.byref(o), ctypes.byref(st)))
+        return _struct_dict(st)
+
+    def mlp_state(self):
+        s = np.zeros(MLP_STATE, np.float32)
+        self._ck(self._L.felog_mlp_get_params(self.h, _addr(s)))
+        return s
+
+    def mlp_set_state(self, state):
+        s = np.ascontiguousarray(state, np.float32)
+        assert s.size == MLP_STATE
+        self._ck(self._L.felog_mlp_set_params(self.h, _addr(s)))
+
+    def mlp_gradient(self, params, X, count, length):
+        p = np.ascontiguousarray(params, np.float32)
+        x = np.ascontiguousarray(X, np.float32)
+        c = np.ascontiguousarray(count, np.uint8)
+        l = np.ascontiguousarray(length, np.float32)
+        g = np.zeros(MLP_PARAMS, np.float32)
+        loss = ctypes.c_double()
+        self._ck(self._L.felog_mlp_gradient(self.h, _addr(p), _addr(x), _addr(c), _addr(l), len(c), _addr(g),
+                                            ctypes.byref(loss)))
+        return g, loss.value
+
+    def mlp_predict(self):
+        n = self.opts.v_num
+        c = np.zeros(n, np.uint8)
+        cf = np.zeros(n, np.float32)
+        l = np.zeros(n, np.float32)
+        self._ck(self._L.felog_mlp_predict(self.h, _addr(c), _addr(cf), _addr(l)))
+        return c, cf, l
 
     def plan(self):
         ns, nsen, nb = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()

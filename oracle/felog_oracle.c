@@ -838,3 +838,109 @@ uint64_t orc_convergence(const float *syn0, const uint32_t *id2offset, int dim, 
   }
   return eva;
 }
+
+/* ---- learned walk budget (this project's; no reference counterpart) ----
+ * Features of vertex v, FP64: log1p(deg), log1p(sum of weights), entropy of
+ * the normalized weights (natural log), log1p(sum of the neighbours'
+ * degrees), log1p(visits), log1p(first walk length). */
+void orc_budget_features(const orc_csr *g, const uint64_t *visits, const uint32_t *first_len, double *feat) {
+  for (uint32_t v = 0; v < g->v_num; v++) {
+    uint64_t b = g->row_ptr[v], e = g->row_ptr[v + 1];
+    double ws = 0, hop2 = 0, h = 0;
+    for (uint64_t i = b; i < e; i++) {
+      ws += (double)g->data[i];
+      uint32_t u = g->nbr[i];
+      hop2 += (double)(g->row_ptr[u + 1] - g->row_ptr[u]);
+    }
+    if (ws > 0)
+      for (uint64_t i = b; i < e; i++) {
+        double p = (double)g->data[i] / ws;
+        if (p > 0) h -= p * log(p);
+      }
+    double *f = feat + (uint64_t)v * 6;
+    f[0] = log1p((double)(e - b));
+    f[1] = log1p(ws);
+    f[2] = h;
+    f[3] = log1p(hop2);
+    f[4] = log1p((double)visits[v]);
+    f[5] = log1p((double)first_len[v]);
+  }
+}
+
+/* MLP 6 -> 64 -> 64 -> (9 + 1), ReLU, parameters W1[64][6] b1 W2[64][64] b2
+ * W3[10][64] b3; loss per sample = softmax cross-entropy of the 9 count logits
+ * against count - 2 plus (out[9] - (length - 50) / 30)^2 / 2.  Mean loss and
+ * mean gradient over n samples, all in FP64. */
+#define MLP_IN 6
+#define MLP_H 64
+#define MLP_C 9
+#define MLP_O 10
+#define MLP_W1 0
+#define MLP_B1 (MLP_W1 + MLP_H * MLP_IN)
+#define MLP_W2 (MLP_B1 + MLP_H)
+#define MLP_B2 (MLP_W2 + MLP_H * MLP_H)
+#define MLP_W3 (MLP_B2 + MLP_H)
+#define MLP_B3 (MLP_W3 + MLP_O * MLP_H)
+#define MLP_P (MLP_B3 + MLP_O)
+
+double orc_mlp_loss_grad(const float *params, const float *X, const uint8_t *count, const float *length, uint64_t n,
+                         double *grad) {
+  double P[MLP_P];
+  for (int i = 0; i < MLP_P; i++) {
+    P[i] = params[i];
+    grad[i] = 0;
+  }
+  double loss = 0;
+  for (uint64_t sidx = 0; sidx < n; sidx++) {
+    double x[MLP_IN], h1[MLP_H], h2[MLP_H], out[MLP_O], d3[MLP_O], d2[MLP_H], d1[MLP_H];
+    for (int i = 0; i < MLP_IN; i++) x[i] = X[sidx * MLP_IN + i];
+    for (int u = 0; u < MLP_H; u++) {
+      double a = P[MLP_B1 + u];
+      for (int i = 0; i < MLP_IN; i++) a += P[MLP_W1 + u * MLP_IN + i] * x[i];
+      h1[u] = a > 0 ? a : 0;
+    }
+    for (int u = 0; u < MLP_H; u++) {
+      double a = P[MLP_B2 + u];
+      for (int k = 0; k < MLP_H; k++) a += P[MLP_W2 + u * MLP_H + k] * h1[k];
+      h2[u] = a > 0 ? a : 0;
+    }
+    for (int c = 0; c < MLP_O; c++) {
+      double a = P[MLP_B3 + c];
+      for (int u = 0; u < MLP_H; u++) a += P[MLP_W3 + c * MLP_H + u] * h2[u];
+      out[c] = a;
+    }
+    double m = out[0], se = 0;
+    for (int c = 1; c < MLP_C; c++) m = out[c] > m ? out[c] : m;
+    for (int c = 0; c < MLP_C; c++) se += exp(out[c] - m);
+    int yc = (int)count[sidx] - 2;
+    double yl = ((double)length[sidx] - 50.0) / 30.0;
+    double dl = out[MLP_C] - yl;
+    loss += log(se) + m - out[yc] + 0.5 * dl * dl;
+    for (int c = 0; c < MLP_C; c++) d3[c] = exp(out[c] - m) / se - (c == yc ? 1.0 : 0.0);
+    d3[MLP_C] = dl;
+    for (int c = 0; c < MLP_O; c++) {
+      for (int u = 0; u < MLP_H; u++) grad[MLP_W3 + c * MLP_H + u] += d3[c] * h2[u];
+      grad[MLP_B3 + c] += d3[c];
+    }
+    for (int u = 0; u < MLP_H; u++) {
+      double d = 0;
+      for (int c = 0; c < MLP_O; c++) d += P[MLP_W3 + c * MLP_H + u] * d3[c];
+      d2[u] = h2[u] > 0 ? d : 0;
+    }
+    for (int u = 0; u < MLP_H; u++) {
+      for (int k = 0; k < MLP_H; k++) grad[MLP_W2 + u * MLP_H + k] += d2[u] * h1[k];
+      grad[MLP_B2 + u] += d2[u];
+    }
+    for (int k = 0; k < MLP_H; k++) {
+      double d = 0;
+      for (int u = 0; u < MLP_H; u++) d += P[MLP_W2 + u * MLP_H + k] * d2[u];
+      d1[k] = h1[k] > 0 ? d : 0;
+    }
+    for (int k = 0; k < MLP_H; k++) {
+      for (int i = 0; i < MLP_IN; i++) grad[MLP_W1 + k * MLP_IN + i] += d1[k] * x[i];
+      grad[MLP_B1 + k] += d1[k];
+    }
+  }
+  for (int i = 0; i < MLP_P; i++) grad[i] /= (double)n;
+  return loss / (double)n;
+}

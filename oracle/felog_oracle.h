@@ -147,6 +147,12 @@ void orc_cbow_bf16(float *syn0, uint16_t *syn0_bf, float *syn1, uint16_t *syn1_b
                    uint32_t sr_seed, const float *exp_table, const int32_t *table, int64_t table_size,
                    long long vocab_size, const int32_t *sen, const uint64_t *sent_start, uint64_t first_sentence,
                    uint64_t n_sentences, int window, int dim, int negative, float alpha);
+/* Learned walk budget (this project's): per-vertex features (V x 6, FP64)
+ * and the MLP's mean loss / gradient over n samples in FP64 (rules in
+ * felog_oracle.c). */
+void orc_budget_features(const orc_csr *g, const uint64_t *visits, const uint32_t *first_len, double *feat);
+double orc_mlp_loss_grad(const float *params, const float *X, const uint8_t *count, const float *length, uint64_t n,
+                         double *grad);
 void orc_cbow_batch(float *syn0, float *syn1, const float *exp_table, const int32_t *table,
                     int64_t table_size, long long vocab_size, const int32_t *sen,
                     const uint64_t *sent_start, uint64_t first_sentence, uint64_t n_sentences,

@@ -87,6 +87,9 @@ def lib():
                                         ctypes.c_uint64, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float]
         L.orc_cbow_bf16.argtypes = L.orc_skipgram_bf16.argtypes
         L.orc_round_sr_seed.argtypes = [ctypes.c_uint64, ctypes.c_uint32]
+        L.orc_budget_features.argtypes = [ctypes.POINTER(Csr), u64p, u32p, f64p]
+        L.orc_mlp_loss_grad.argtypes = [f32p, f32p, ctypes.POINTER(ctypes.c_uint8), f32p, ctypes.c_uint64, f64p]
+        L.orc_mlp_loss_grad.restype = ctypes.c_double
         L.orc_round_sr_seed.restype = ctypes.c_uint32
         L.orc_convergence.argtypes = [f32p, u32p, ctypes.c_int, ctypes.POINTER(Csr), u8p, ctypes.c_uint64,
                                       ctypes.c_uint32, f32p]
@@ -261,6 +264,25 @@ def skipgram_bf16(m0, m1, sr_seed, exp_tab, table, vocab_size, sen, sent_start, 
        ptr(exp_tab, f32p), ptr(table, i32p), len(table), vocab_size,
        ptr(np.ascontiguousarray(sen, np.int32), i32p), ptr(np.ascontiguousarray(sent_start, np.uint64), u64p),
        first, n, window, dim, negative, alpha)
+
+
+def budget_features(csr, visits, first_len):
+    v = np.ascontiguousarray(visits, np.uint64)
+    fl = np.ascontiguousarray(first_len, np.uint32)
+    out = np.zeros(csr.c.v_num * 6, np.float64)
+    lib().orc_budget_features(ctypes.byref(csr.c), ptr(v, u64p), ptr(fl, u32p), ptr(out, f64p))
+    return out.reshape(-1, 6)
+
+
+def mlp_loss_grad(params, X, count, length):
+    p = np.ascontiguousarray(params, np.float32)
+    x = np.ascontiguousarray(X, np.float32)
+    c = np.ascontiguousarray(count, np.uint8)
+    l = np.ascontiguousarray(length, np.float32)
+    g = np.zeros(5258, np.float64)
+    loss = lib().orc_mlp_loss_grad(ptr(p, f32p), ptr(x, f32p), c.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)),
+                                   ptr(l, f32p), len(c), ptr(g, f64p))
+    return g, loss
 
 
 def negreuse_batch(syn0, syn1, exp_tab, sen, sent_start, first, n, negs, window, dim, negative, alpha):

@@ -45,7 +45,7 @@ def test_create_reports_status_without_crashing():
     assert st in (0, 3)
     if st == 0:
         L.felog_destroy(h)
-    assert L.felog_abi_version() == 1
+    assert L.felog_abi_version() == 2
 
 
 def test_synth_graph_contract():
