@@ -49,6 +49,8 @@ CONFIGS = {
 }
 TRAIN = dict(min_length=20, min_rounds=2, size=128, window=10, negative=5, sample=1e-3, cbow=0, reuse_neg=0,
              min_count=0)
+FORMS = {"plain-fp32": dict(precision=0, budget_mode=0), "learned-bf16": dict(precision=1, budget_mode=1)}
+BUDGET_MODEL = os.path.join(ROOT, "info-centric_ge_b200", "felog_b200", "budget_mlp_c4.npy")
 METRIC = "walk+SGNS corpus tokens/s (walk steps/s and SGNS words/s reported alongside)"
 WALK_BYTES_PER_STEP = 68      # 2 random 32-B sectors + 4-B token write
 SGNS_BYTES_PER_PAIR = {"fp32": 7168,   # 14 rows x 128 x 4 B (read + write syn0 row and 6 syn1 rows)
@@ -164,6 +166,8 @@ def sum_over_ranks(pg, x):
 
 def run_round(f, r, min_rounds, counters):
     ws = f.walk_round(r)
+    if f.opts.budget_mode == 1 and r == 0:
+        f.mlp_predict()  # learned budget: features from the first round's walks
     ts = f.train_round(r)
     counters["tokens"] += ws["n_tokens"]
     counters["words"] += ts["words"]
@@ -211,16 +215,66 @@ def cpu_baseline(g, cfg):
             "walk_steps_per_s": walk_rate, "sgns_words_per_s": train_rate}
 
 
+def new_context(fb, g, form, device, seed, model):
+    V = g["v_num"]
+    f = fb.Felog(v_num=V, device=device, seed=seed, **FORMS[form], **TRAIN)
+    f.load_graph(g["edges"], V)
+    f.init_model()
+    if FORMS[form]["budget_mode"] == 1:
+        f.mlp_set_state(model)
+    return f
+
+
+def link_auc(f, g):
+    """Exact AUC of the held-out edges against the sampled non-edges, scored by
+    the cosine of the two endpoints' syn0 rows (FP64 on the host)."""
+    import felog_b200 as fb
+    s0, _ = f.embeddings()
+    _, id2, vs, _ = f.vocab()
+    e0 = s0.reshape(vs, -1)[id2]
+    del s0
+    def score(e):
+        e = e / np.maximum(np.linalg.norm(e, axis=1, keepdims=True), 1e-30)
+        cos = np.einsum("ij,ij->i", e[g["test_src"]], e[g["test_dst"]])
+        return float(fb.auc(cos.astype(np.float64), g["test_label"]))
+    raw = score(e0)
+    # the same cosine after removing the mean row (the direction that rarely
+    # trained rows share), for information
+    centered = score(e0 - e0.mean(axis=0, keepdims=True))
+    return raw, centered
+
+
+def compare_forms(fb, g, device, model):
+    """Plain FP32 and learned-budget BF16, each run end to end (felog_run: walk,
+    train and budget check until the stop-all rule) on the same graph and walk
+    seed; job time is the device time of the whole run."""
+    out = {}
+    for form in ("plain-fp32", "learned-bf16"):
+        f = new_context(fb, g, form, device, 77, model)
+        t0 = time.perf_counter()
+        rs = f.run()
+        wall = time.perf_counter() - t0
+        out[form] = {"rounds": rs["rounds"], "walk_tokens": rs["walk_tokens"], "train_words": rs["train_words"],
+                     "job_ms": rs["total_ms"], "wall_ms": wall * 1e3,
+                     "tokens_per_s": rs["walk_tokens"] / (rs["total_ms"] * 1e-3)}
+        out[form]["auc"], out[form]["auc_centered"] = link_auc(f, g)
+        f.close()
+    p, l = out["plain-fp32"], out["learned-bf16"]
+    out["end_to_end_speedup"] = p["job_ms"] / l["job_ms"]
+    out["auc_delta"] = l["auc"] - p["auc"]
+    return out
+
+
 def bench_mine(args):
     import felog_b200 as fb
     world, rank, local, pg = dist_setup(args)
     cfg = CONFIGS[args.config]
     g = make_graph(cfg)
     V = g["v_num"]
-    prec = args.precision
-    f = fb.Felog(v_num=V, device=local, seed=1000 + rank, precision=1 if prec == "bf16" else 0, **TRAIN)
-    f.load_graph(g["edges"], V)
-    f.init_model()
+    form = args.form
+    prec = "bf16" if FORMS[form]["precision"] else "fp32"
+    model = np.load(args.budget_model) if FORMS[form]["budget_mode"] or not args.no_forms else None
+    f = new_context(fb, g, form, local, 1000 + rank, model)
     min_r = TRAIN["min_rounds"]
     warm = {k: 0.0 for k in ("tokens", "words", "pairs", "walk_ms", "train_ms", "plan_ms", "budget_ms")}
     for r in range(args.warmup):
@@ -280,7 +334,7 @@ def bench_mine(args):
         "dtype": ("f32 tables" if prec == "fp32" else "bf16 tables (f32 master rows for the top 1%), f32 arithmetic")
                  + ", f64 walk statistics",
         "data": "synthetic (seeded R-MAT, see config)",
-        "config": {"workload": cfg["workload"] if prec == "fp32" else cfg["workload"].replace("plain FP32", "BF16 form"),
+        "config": {"workload": cfg["workload"].replace("plain FP32", form), "form": form,
                    "v_num": V, "train_edges": int(len(g["edges"])),
                    "dim": 128, "window": 10, "negative": 5, "sample": 1e-3, "min_L": 20, "min_R": 2,
                    "skip_gram": True, "reuse_neg": 0, "precision": prec,
@@ -301,6 +355,8 @@ def bench_mine(args):
         "gpu_launches": int(launches),
         "clocks": clk.summary(),
     }
+    if rank == 0 and world == 1 and not args.no_forms:
+        out["forms"] = compare_forms(fb, g, local, model)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             out["cpu_baseline"] = cpu_baseline(g, cfg)
@@ -363,7 +419,9 @@ def main():
     ap.add_argument("--config", default="c2", choices=sorted(CONFIGS))
     ap.add_argument("--ref-walkers", type=int, default=200000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--precision", default="fp32", choices=["fp32", "bf16"])
+    ap.add_argument("--form", default="learned-bf16", choices=sorted(FORMS))
+    ap.add_argument("--budget-model", default=BUDGET_MODEL)
+    ap.add_argument("--no-forms", action="store_true", help="skip the end-to-end plain vs learned comparison")
     args = ap.parse_args()
     if args.impl == "reference":
         bench_reference(args)
