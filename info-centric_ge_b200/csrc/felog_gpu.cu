@@ -1051,6 +1051,8 @@ felog_status train_pairs(felog_ctx *c, SgArgs g, int blocks, int threads) {
   CK(c->pr_cfirst.ensure(c->plan_sen + 1), "train: center offsets");
   pa.cstate = c->pr_cstate.p;
   pa.cfirst = c->pr_cfirst.p;
+  pa.reuse = c->o.reuse_neg ? 1 : 0;
+  pa.negs = c->p_negs.p;
   pa.count = c->pr_count.p;
   pa.off = c->pr_off.p;
   CK(cudaMemsetAsync(c->pr_count.p + n, 0, 8, c->stream), "train");
@@ -1117,7 +1119,9 @@ extern "C" felog_status felog_train_round(felog_ctx *c, uint32_t round, float al
   if (!c) return FELOG_INVALID_ARG;
   if (!c->model_ready) return fail(c, FELOG_NOT_READY, "model not initialised");
   if (!c->corpus_ready) return fail(c, FELOG_NOT_READY, "no corpus");
-  if (c->o.reuse_neg) return fail(c, FELOG_INVALID_ARG, "-reuse-neg 1 training is not available in this build");
+  // -reuse-neg applies to skip-gram only; with -cbow 1 the CBOW kernel runs (word2vec.cu:1255-1258)
+  if (c->o.reuse_neg && !c->o.cbow && (c->o.size < 64 || (c->o.negative != 5 && c->o.negative != 7)))
+    return fail(c, FELOG_INVALID_ARG, "-reuse-neg 1 runs skip-gram with -negative 5 or 7 and -size >= 64");
   CK(cudaSetDevice(c->device), "train_round");
   if (alpha < 0) alpha = schedule_alpha(c, round);
   float ms_plan = 0, ms_train = 0;

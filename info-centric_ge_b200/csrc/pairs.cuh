@@ -9,6 +9,8 @@
 //     1e8], 0 -> next % (vocab - 1) + 1, skipped when equal to the word
 //     (:496-507);
 // with next seeded by the sentence's index in its batch (blockIdx.x, :446).
+// With -reuse-neg 1 (__sgNegReuse, word2vec.cu:368-440) the window is the full
+// window and the K negatives are the sentence's plan negatives.
 // The draws depend only on the plan, never on the rows, so one scalar thread
 // per sentence produces them ahead of training; the trainer's warps then do
 // row work only.
@@ -45,6 +47,8 @@ struct PairArgs {
   unsigned long long *cstate;  // per center (plan token): LCG state after its window draw
   uint32_t *cfirst;            // per center: pairs of its sentence before it
   const unsigned long long *jump_a, *jump_c;  // the negative LCG advanced by K j steps, j < 2 window
+  int reuse;             // -reuse-neg 1: full window, negatives from negs
+  const int32_t *negs;   // plan negatives, K per sentence
 };
 
 // number of valid contexts of the center at pos with window shrink b
@@ -63,13 +67,16 @@ __global__ void k_pair_count(PairArgs a) {
     unsigned long long nr = a.blk[s];
     uint64_t n = 0;
     for (long long pos = sb; pos < se; pos++) {
-      nr = nr * 2514903917ULL + 11ULL;
-      const int b = (int)fastmod(nr, a.fm_window);
+      int b = 0;
+      if (!a.reuse) {
+        nr = nr * 2514903917ULL + 11ULL;
+        b = (int)fastmod(nr, a.fm_window);
+      }
       const int c = contexts_of(pos, sb, se, a.window, b);
       a.cstate[pos] = nr;
       a.cfirst[pos] = (uint32_t)n;
       n += (uint64_t)c;
-      if (c) nr = a.jump_a[c] * nr + a.jump_c[c];
+      if (c && !a.reuse) nr = a.jump_a[c] * nr + a.jump_c[c];
     }
     a.count[s] = n;
   }
@@ -126,7 +133,7 @@ __global__ void __launch_bounds__(256) k_pair_emit(PairArgs a) {
         const uint64_t p = p0 + lane + 32 * u;
         const uint32_t j = live[u] ? (uint32_t)(p - a.cfirst[pos[u]]) : 0u;
         nr[u] = a.cstate[pos[u]];
-        const int b = (int)fastmod(nr[u], a.fm_window);
+        const int b = a.reuse ? 0 : (int)fastmod(nr[u], a.fm_window);
         long long c = pos[u] - a.window + b;
         if (c < sb) c = sb;
         c += j;
@@ -134,17 +141,24 @@ __global__ void __launch_bounds__(256) k_pair_emit(PairArgs a) {
         if (c >= se) c = se - 1;  // only for lanes past the end (not written)
         word[u] = a.sen[pos[u]];
         ctx[u] = a.sen[c];
-        nr[u] = a.jump_a[j] * nr[u] + a.jump_c[j];
+        if (!a.reuse) nr[u] = a.jump_a[j] * nr[u] + a.jump_c[j];
       }
       int32_t t[U][K];
+      if (a.reuse) {
 #pragma unroll
-      for (int q = 0; q < K; q++)
+        for (int q = 0; q < K; q++)
 #pragma unroll
-        for (int u = 0; u < U; u++) {
-          nr[u] = nr[u] * 25214903917ULL + 11ULL;
-          t[u][q] = __ldg(&a.table[(nr[u] >> 16) % kUnigramSlots]);
-          if (t[u][q] == 0) t[u][q] = -2 - (int)fastmod(nr[u], a.fm_vocab1);  // fallback, resolved below
-        }
+          for (int u = 0; u < U; u++) t[u][q] = __ldg(&a.negs[s * (uint64_t)K + q]);
+      } else {
+#pragma unroll
+        for (int q = 0; q < K; q++)
+#pragma unroll
+          for (int u = 0; u < U; u++) {
+            nr[u] = nr[u] * 25214903917ULL + 11ULL;
+            t[u][q] = __ldg(&a.table[(nr[u] >> 16) % kUnigramSlots]);
+            if (t[u][q] == 0) t[u][q] = -2 - (int)fastmod(nr[u], a.fm_vocab1);  // fallback, resolved below
+          }
+      }
 #pragma unroll
       for (int u = 0; u < U; u++) {
         if (!live[u]) continue;

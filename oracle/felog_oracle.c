@@ -448,19 +448,21 @@ void orc_skipgram_batch(float *syn0, float *syn1, const float *exp_table, const 
   }
 }
 
-/* plain sequential dot for the reuse-neg algorithm (true dot product) */
-static float seq_dot(const float *x, const float *y, int dim) {
-  float f = 0;
-  for (int t = 0; t < dim; t++) f = fmaf(x[t], y[t], f);
-  return f;
-}
-
+/* __sgNegReuse (word2vec.cu:368-440) restated with a true dot product: per
+ * sentence K negatives drawn by the host plan, the full window (no shrink), and
+ * for every (center, context) pair the positive (the center word) and the
+ * negatives not equal to it.  The reference's warp reduction
+ * (reduceInWarp, word2vec.cu:214-219, __shfl_sync(f, i) reads lane i) does not
+ * form a dot product; here each score is the skip-gram tree dot.  Targets are
+ * taken in the order positive, negative 0..K-1, each scored against the rows
+ * as they are at that point (targets with distinct rows do not see each
+ * other's updates, as in the reference where all K + 1 warps score before
+ * they update); sigma is the expTable lookup (the reference recomputes the
+ * same quantized sigmoid with exp). */
 void orc_negreuse_batch(float *syn0, float *syn1, const float *exp_table, const int32_t *sen,
                         const uint64_t *sent_start, uint64_t first_sentence, uint64_t n_sentences,
                         const int32_t *negs, int window, int dim, int negative, float alpha) {
   float neu1e[512];
-  float g[64];
-  int tgt[64];
   for (uint64_t blk = 0; blk < n_sentences; blk++) {
     uint64_t s = first_sentence + blk;
     long long ss = (long long)sent_start[s], se = (long long)sent_start[s + 1];
@@ -473,23 +475,18 @@ void orc_negreuse_batch(float *syn0, float *syn1, const float *exp_table, const 
         long long c = pos - window + a;
         if (c < ss || c >= se || sen[c] == -1) continue;
         float *x = syn0 + (long long)sen[c] * dim;
-        int nt = 0;
-        for (int y = 0; y <= negative; y++) { /* warp y < K: negative y, warp K: positive */
-          int target = y == negative ? word : neg[y];
-          if (y < negative && target == word) continue;
-          int label = y == negative ? 1 : 0;
-          float f = seq_dot(x, syn1 + (long long)target * dim, dim);
-          g[nt] = sg_gradient(f, label, exp_table, alpha);
-          tgt[nt++] = target;
-        }
         for (int t = 0; t < dim; t++) neu1e[t] = 0;
-        for (int k = 0; k < nt; k++) {
-          float *yv = syn1 + (long long)tgt[k] * dim;
-          for (int t = 0; t < dim; t++) neu1e[t] = fmaf(g[k], yv[t], neu1e[t]);
-        }
-        for (int k = 0; k < nt; k++) {
-          float *yv = syn1 + (long long)tgt[k] * dim;
-          for (int t = 0; t < dim; t++) yv[t] += g[k] * x[t];
+        for (int d = 0; d <= negative; d++) {
+          int target = d == 0 ? word : neg[d - 1];
+          if (d > 0 && target == word) continue;
+          int label = d == 0 ? 1 : 0;
+          float *y = syn1 + (long long)target * dim;
+          float f = sg_dot(x, y, dim);
+          float g = sg_gradient(f, label, exp_table, alpha);
+          for (int t = 0; t < dim; t++) {
+            neu1e[t] = fmaf(g, y[t], neu1e[t]);
+            y[t] += g * x[t];
+          }
         }
         for (int t = 0; t < dim; t++) x[t] += neu1e[t];
       }
@@ -633,11 +630,13 @@ uint32_t orc_round_sr_seed(uint64_t seed, uint32_t round) {
   return sr_h((uint32_t)seed ^ sr_h((uint32_t)(seed >> 32) + round * 0x9E3779B9u));
 }
 
-void orc_skipgram_bf16(float *syn0, uint16_t *syn0_bf, float *syn1, uint16_t *syn1_bf, long long n_hot,
-                       uint32_t sr_seed, const float *exp_table, const int32_t *table, int64_t table_size,
-                       long long vocab_size, const int32_t *sen, const uint64_t *sent_start,
-                       uint64_t first_sentence, uint64_t n_sentences, int window, int dim, int negative,
-                       float alpha) {
+/* negs == NULL: skip_gram_kernel draws; else __sgNegReuse (full window, the
+ * sentence's plan negatives) as in orc_negreuse_batch */
+static void sg_bf16_impl(float *syn0, uint16_t *syn0_bf, float *syn1, uint16_t *syn1_bf, long long n_hot,
+                         uint32_t sr_seed, const float *exp_table, const int32_t *table, int64_t table_size,
+                         long long vocab_size, const int32_t *sen, const uint64_t *sent_start,
+                         uint64_t first_sentence, uint64_t n_sentences, int window, int dim, int negative,
+                         float alpha, const int32_t *negs) {
   mixed_rows m0 = {syn0, syn0_bf, n_hot, dim}, m1 = {syn1, syn1_bf, n_hot, dim};
   float x[512], y[512], neu1e[512], upd[512];
   for (uint64_t blk = 0; blk < n_sentences; blk++) {
@@ -648,8 +647,11 @@ void orc_skipgram_bf16(float *syn0, uint16_t *syn0_bf, float *syn1, uint16_t *sy
     for (long long pos = ss; pos < se; pos++) {
       int word = sen[pos];
       if (word == -1) continue;
-      next_random = next_random * (unsigned long)2514903917 + 11;
-      int b = (int)(next_random % (unsigned long)window);
+      int b = 0;
+      if (!negs) {
+        next_random = next_random * (unsigned long)2514903917 + 11;
+        b = (int)(next_random % (unsigned long)window);
+      }
       for (int a = b; a < window * 2 + 1 - b; a++) {
         if (a == window) continue;
         long long c = pos - window + a;
@@ -664,6 +666,10 @@ void orc_skipgram_bf16(float *syn0, uint16_t *syn0_bf, float *syn1, uint16_t *sy
           if (d == 0) {
             target = word;
             label = 1;
+          } else if (negs) {
+            target = negs[s * (uint64_t)negative + d - 1];
+            if (target == word) continue;
+            label = 0;
           } else {
             next_random = next_random * (unsigned long)25214903917 + 11;
             target = table[(next_random >> 16) % (unsigned long)table_size];
@@ -684,6 +690,23 @@ void orc_skipgram_bf16(float *syn0, uint16_t *syn0_bf, float *syn1, uint16_t *sy
       }
     }
   }
+}
+
+void orc_skipgram_bf16(float *syn0, uint16_t *syn0_bf, float *syn1, uint16_t *syn1_bf, long long n_hot,
+                       uint32_t sr_seed, const float *exp_table, const int32_t *table, int64_t table_size,
+                       long long vocab_size, const int32_t *sen, const uint64_t *sent_start,
+                       uint64_t first_sentence, uint64_t n_sentences, int window, int dim, int negative,
+                       float alpha) {
+  sg_bf16_impl(syn0, syn0_bf, syn1, syn1_bf, n_hot, sr_seed, exp_table, table, table_size, vocab_size, sen,
+               sent_start, first_sentence, n_sentences, window, dim, negative, alpha, NULL);
+}
+
+void orc_negreuse_bf16(float *syn0, uint16_t *syn0_bf, float *syn1, uint16_t *syn1_bf, long long n_hot,
+                       uint32_t sr_seed, const float *exp_table, const int32_t *sen, const uint64_t *sent_start,
+                       uint64_t first_sentence, uint64_t n_sentences, const int32_t *negs, int window, int dim,
+                       int negative, float alpha) {
+  sg_bf16_impl(syn0, syn0_bf, syn1, syn1_bf, n_hot, sr_seed, exp_table, NULL, 0, 0, sen, sent_start, first_sentence,
+               n_sentences, window, dim, negative, alpha, negs);
 }
 
 void orc_cbow_bf16(float *syn0, uint16_t *syn0_bf, float *syn1, uint16_t *syn1_bf, long long n_hot,

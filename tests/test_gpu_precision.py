@@ -77,6 +77,34 @@ def test_bf16_deterministic_matches_oracle(dim, negative, cbow):
     assert exact == (1.0, 1.0), f"fraction bit-exact syn0/syn1: {exact}"
 
 
+@pytest.mark.parametrize("dim", [128, 64])
+def test_bf16_reuse_neg_deterministic_matches_oracle(dim):
+    e, V = graph4096()
+    f = fb.Felog(v_num=V, size=dim, window=5, negative=5, sample=1e-3, cbow=0, reuse_neg=1, min_count=0,
+                 precision=1, deterministic=1, seed=SEED)
+    f.load_graph(e, V)
+    f.init_model()
+    _, _, vs, _ = f.vocab()
+    nh = n_hot(vs)
+    o0, o1 = ob.init_net(vs, dim)
+    m0, m1 = ob.MixedRows(o0, vs, dim, nh), ob.MixedRows(o1, vs, dim, nh)
+    tok, off = walk_corpus(V, e, 300, seed=4)
+    f.set_corpus(tok, off)
+    f.train_round(0, alpha=0.025)
+    c = ob.OracleCsr(e, V)
+    vv, vcn, id2, _, tw = ob.vocab(c.deg, 0)
+    thr, used = ob.subsample_thresholds(vcn, 1e-3, tw)
+    table = ob.unigram_table(vcn)
+    pl = ob.plan_batches(tok, off, id2, thr, used, table, vs, 5)
+    bf = pl["batch_first"]
+    for b in range(len(bf) - 1):
+        ob.negreuse_bf16(m0, m1, ob.round_sr_seed(SEED, 0), ob.exp_table(), pl["sen"], pl["sent_start"], int(bf[b]),
+                         int(bf[b + 1] - bf[b]), pl["negs"], 5, dim, 5, 0.025)
+    g0, g1 = f.embeddings()
+    exact = np.mean(g0 == m0.full()), np.mean(g1 == m1.full())
+    assert exact == (1.0, 1.0), f"fraction bit-exact syn0/syn1: {exact}"
+
+
 def link_auc(s0, id2, vs, dim, g):
     e0 = s0.reshape(vs, dim)[id2]
     n0 = e0 / np.maximum(np.linalg.norm(e0, axis=1, keepdims=True), 1e-30)

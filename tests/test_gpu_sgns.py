@@ -32,9 +32,9 @@ def graph4096():
     return fx["edges"], int(fx["V"])
 
 
-def trainer(dim=128, window=10, negative=5, sample=1e-3, **kw):
+def trainer(dim=128, window=10, negative=5, sample=1e-3, reuse_neg=0, **kw):
     e, V = graph4096()
-    f = fb.Felog(v_num=V, size=dim, window=window, negative=negative, sample=sample, cbow=0, reuse_neg=0,
+    f = fb.Felog(v_num=V, size=dim, window=window, negative=negative, sample=sample, cbow=0, reuse_neg=reuse_neg,
                  min_count=0, **kw)
     f.load_graph(e, V)
     f.init_model()
@@ -203,3 +203,31 @@ def test_hogwild_auc_within_0005_of_sequential_oracle():
     # convergence check); the syn0 . syn1 score is printed for information
     print("AUC cosine / syn0.syn1: gpu", a_gpu, "oracle", a_orc)
     assert abs(a_gpu[0] - a_orc[0]) < 0.005, (a_gpu, a_orc)
+
+
+@pytest.mark.parametrize("dim,negative", [(128, 5), (64, 7), (256, 5)])
+def test_reuse_neg_deterministic_matches_oracle(dim, negative):
+    """-reuse-neg 1 (per-sentence plan negatives, full window) in the one-warp
+    mode equals the oracle's restatement of __sgNegReuse with true dots."""
+    f, e, V = trainer(dim=dim, window=5, negative=negative, sample=1e-3, deterministic=1, reuse_neg=1)
+    tok, off = walk_corpus(V, e, seed=9)
+    n = 300
+    tok, off = tok[: int(off[n])], off[: n + 1]
+    f.set_corpus(tok, off)
+    f.train_round(0, alpha=0.025)
+    g0, g1 = f.embeddings()
+    c = ob.OracleCsr(e, V)
+    vv, vcn, id2, vs, tw = ob.vocab(c.deg, 0)
+    thr, used = ob.subsample_thresholds(vcn, 1e-3, tw)
+    table = ob.unigram_table(vcn)
+    et = ob.exp_table()
+    syn0, syn1 = ob.init_net(vs, dim)
+    pl = ob.plan_batches(tok, off, id2, thr, used, table, vs, negative)
+    gp = f.plan()
+    assert np.array_equal(gp["negs"], pl["negs"])
+    bf = pl["batch_first"]
+    for b in range(len(bf) - 1):
+        ob.negreuse_batch(syn0, syn1, et, pl["sen"], pl["sent_start"], int(bf[b]), int(bf[b + 1] - bf[b]),
+                          pl["negs"], 5, dim, negative, 0.025)
+    exact = np.mean(g0 == syn0), np.mean(g1 == syn1)
+    assert exact == (1.0, 1.0), f"fraction bit-exact syn0/syn1: {exact}"
