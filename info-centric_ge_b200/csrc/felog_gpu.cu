@@ -94,6 +94,7 @@ struct felog_ctx {
   DevBuf<unsigned int> visit_freq;
   uint64_t words_sum_cum = 0;
   DevBuf<unsigned long long> counters;  // scratch counters
+  DevBuf<unsigned int> walk_claim;     // walker claim counters
   DevBuf<int> derr;
   DevBuf<uint64_t> inj_idx_off, inj_p_off;
   DevBuf<uint32_t> inj_idx;
@@ -289,7 +290,7 @@ extern "C" void felog_destroy(felog_ctx *c) {
   c->exp_table.release(); c->syn0.release(); c->syn1.release(); c->syn0_bf.release(); c->syn1_bf.release(); c->jump.release();
   c->p_cand.release(); c->p_draws.release(); c->p_cons.release(); c->p_kept.release(); c->p_blk.release();
   c->p_state.release(); c->p_neg_state.release(); c->p_out_off.release(); c->p_batch_first.release();
-  c->p_sen.release(); c->pr_count.release(); c->pr_off.release(); c->pr_rec.release(); c->pr_cstate.release(); c->pr_jump.release(); c->pr_cfirst.release(); c->p_negs.release(); c->sim.release(); c->bud_walks.release(); c->bud_len_sum.release(); c->bud_first_len.release(); c->bud_stop_round.release(); c->feat.release(); c->mlp_params.release(); c->mlp_m1.release(); c->mlp_m2.release(); c->mlp_partial.release(); c->mlp_norm.release(); c->mlp_grad.release(); c->pred_conf.release(); c->pred_len.release(); c->mlp_loss.release(); c->mlp_idx.release(); c->mlp_ycount.release(); c->pred_count.release(); c->mlp_ylen.release(); c->cub_tmp.release(); c->out_tmp.release();
+  c->p_sen.release(); c->walk_claim.release(); c->pr_count.release(); c->pr_off.release(); c->pr_rec.release(); c->pr_cstate.release(); c->pr_jump.release(); c->pr_cfirst.release(); c->p_negs.release(); c->sim.release(); c->bud_walks.release(); c->bud_len_sum.release(); c->bud_first_len.release(); c->bud_stop_round.release(); c->feat.release(); c->mlp_params.release(); c->mlp_m1.release(); c->mlp_m2.release(); c->mlp_partial.release(); c->mlp_norm.release(); c->mlp_grad.release(); c->pred_conf.release(); c->pred_len.release(); c->mlp_loss.release(); c->mlp_idx.release(); c->mlp_ycount.release(); c->pred_count.release(); c->mlp_ylen.release(); c->cub_tmp.release(); c->out_tmp.release();
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
   if (c->tm0) cudaEventDestroy(c->tm0);
@@ -622,13 +623,17 @@ extern "C" felog_status felog_walk_round(felog_ctx *c, uint32_t round, const fel
   a.sent_len = c->sent_len.p;
   a.visit_freq = c->visit_freq.p;
   a.corr_tab = c->corr_tab.p;
-  a.next_walker = reinterpret_cast<unsigned int *>(c->counters.p + 9);
+  CK(c->walk_claim.ensure(kWalkClaimers), "walk_round");
+  CK(cudaMemsetAsync(c->walk_claim.p, 0, 4 * kWalkClaimers, c->stream), "walk_round");
+  a.next_walker = c->walk_claim.p;
   a.stats = c->counters.p;
   a.err = c->derr.p;
   CK(cudaEventRecord(c->ev0, c->stream), "walk_round");
   if (na) {
     int blocks = c->sm_count * 8;
-    k_walk<<<blocks, 256, 0, c->stream>>>(a);
+    if (a.injected) k_walk<true, false><<<blocks, 256, 0, c->stream>>>(a);
+    else if (a.weighted) k_walk<false, true><<<blocks, 256, 0, c->stream>>>(a);
+    else k_walk<false, false><<<blocks, 256, 0, c->stream>>>(a);
     c->launches++;
     CK(cudaGetLastError(), "walk_round: launch");
   }

@@ -54,10 +54,12 @@ struct WalkArgs {
   uint32_t *sent_len;
   unsigned int *visit_freq;      // cumulative visits per vertex (KL)
   const double *corr_tab;        // t(S, fi) table (k_corr_table), or NULL
-  unsigned int *next_walker;
+  unsigned int *next_walker;     // kWalkClaimers claim counters (walker i + kWalkClaimers j)
   unsigned long long *stats;     // [tokens, traces, iterations, long]
   int *err;
 };
+
+constexpr uint32_t kWalkClaimers = 64;  // claim counters: walkers i, i + 64, i + 128, ... share counter i
 
 struct Corr {
   double H, EH, ES, EHS, EHH, ESS, R, S;  // N == S throughout (both count tokens)
@@ -157,10 +159,15 @@ __device__ __forceinline__ bool path_push(const WalkArgs &a, PathBuf &pb, uint32
   return true;
 }
 
+// INJ: parity mode with injected draws; WEIGHTED: alias-table candidates.
+template <bool INJ, bool WEIGHTED>
 __global__ void __launch_bounds__(256, 3) k_walk(WalkArgs a) {
   unsigned long long my_tok = 0, my_tr = 0, my_it = 0, my_long = 0;
+  // walkers are claimed through kWalkClaimers counters so that claims do not
+  // serialize on one address
+  const uint32_t claimer = (blockIdx.x * blockDim.x + threadIdx.x) % kWalkClaimers;
   for (;;) {
-    uint32_t k = atomicAdd(a.next_walker, 1u);
+    const uint32_t k = claimer + kWalkClaimers * atomicAdd(&a.next_walker[claimer], 1u);
     if (k >= a.n_active) break;
     const uint32_t w = a.active[k];
     const uint32_t start = w % a.v_num, replica = w / a.v_num;
@@ -174,7 +181,7 @@ __global__ void __launch_bounds__(256, 3) k_walk(WalkArgs a) {
     uint32_t step = 0, iter = 0, cnt_cur = 1;
     uint64_t bloom = bloom_bit(start);
     uint64_t di = 0, di_end = 0, dp = 0, dp_end = 0;
-    if (a.injected) {
+    if (INJ) {
       di = a.inj_idx_off[k];
       di_end = a.inj_idx_off[k + 1];
       dp = a.inj_p_off[k];
@@ -184,7 +191,7 @@ __global__ void __launch_bounds__(256, 3) k_walk(WalkArgs a) {
       if (deg == 0) break;
       uint32_t r;
       double p = 0.0;
-      if (a.injected) {
+      if (INJ) {
         if (di >= di_end) {
           set_error(a.err, kErrDrawsExhausted);
           break;
@@ -196,7 +203,7 @@ __global__ void __launch_bounds__(256, 3) k_walk(WalkArgs a) {
         }
       } else {
         walk_draw(a.seed, start, a.round, iter, replica, deg, r, p);
-        if (a.weighted) {
+        if (WEIGHTED) {
           // alias draw: keep slot r with probability prob[r], else take its
           // alias; the coin comes from a second Philox block of this iteration.
           uint4 o = philox4x32_10(make_uint4(start, a.round, iter, replica ^ 0x80000000u),
@@ -213,7 +220,7 @@ __global__ void __launch_bounds__(256, 3) k_walk(WalkArgs a) {
       if (deg == 2 && a.adj[b].x == cur) break;
       const uint2 cand = a.adj[b + r];
       if (step == 0 && cand.x == cur) continue;
-      if (a.injected) {
+      if (INJ) {
         if (dp >= dp_end) {
           set_error(a.err, kErrDrawsExhausted);
           break;
