@@ -25,6 +25,7 @@ engine with all host threads and its CUDA skip-gram kernels.
 import argparse
 import json
 import os
+import re
 import statistics
 import subprocess
 import sys
@@ -392,7 +393,14 @@ def bench_reference(args):
         print(json.dumps({"impl": "reference", "unavailable": f"ref_pipeline exited {res.returncode}: "
                                                               f"{res.stderr.strip()[-200:]}"}))
         return
-    d = json.loads(res.stdout.strip().splitlines()[-1])
+    # the reference's progress output ends in carriage returns, so the result
+    # may share a line with it
+    lines = re.findall(r'\{"tokens".*?\}', res.stdout)
+    if not lines:
+        print(json.dumps({"impl": "reference", "unavailable": "ref_pipeline printed no result line: "
+                                                              f"{res.stdout.strip()[-200:]}"}))
+        return
+    d = json.loads(lines[-1])
     value = d["tokens"] / d["seconds"]
     out = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "tokens/s", "n_gpus": world,
@@ -417,7 +425,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
     ap.add_argument("--config", default="c2", choices=sorted(CONFIGS))
-    ap.add_argument("--ref-walkers", type=int, default=200000)
+    ap.add_argument("--ref-walkers", type=int, default=0,
+                    help="walkers of the reference arm (0: one per vertex; the reference asserts every vertex is visited)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--form", default="learned-bf16", choices=sorted(FORMS))
     ap.add_argument("--budget-model", default=BUDGET_MODEL)

@@ -111,6 +111,7 @@ struct felog_ctx {
   DevBuf<uint16_t> thr;
   bool use_thr = false;
   DevBuf<int32_t> table;
+  DevBuf<uint32_t> table_coarse;  // per 64-slot bucket: first word, top bit when uniform
   DevBuf<float> exp_table;
   DevBuf<float> syn0, syn1;        // FP32 rows 0..n_f32-1 (all rows in FP32 mode)
   DevBuf<uint16_t> syn0_bf, syn1_bf;  // BF16 mode: rows n_f32.. as BF16 bits
@@ -290,7 +291,7 @@ extern "C" void felog_destroy(felog_ctx *c) {
   c->exp_table.release(); c->syn0.release(); c->syn1.release(); c->syn0_bf.release(); c->syn1_bf.release(); c->jump.release();
   c->p_cand.release(); c->p_draws.release(); c->p_cons.release(); c->p_kept.release(); c->p_blk.release();
   c->p_state.release(); c->p_neg_state.release(); c->p_out_off.release(); c->p_batch_first.release();
-  c->p_sen.release(); c->walk_claim.release(); c->pr_count.release(); c->pr_off.release(); c->pr_rec.release(); c->pr_cstate.release(); c->pr_jump.release(); c->pr_cfirst.release(); c->p_negs.release(); c->sim.release(); c->bud_walks.release(); c->bud_len_sum.release(); c->bud_first_len.release(); c->bud_stop_round.release(); c->feat.release(); c->mlp_params.release(); c->mlp_m1.release(); c->mlp_m2.release(); c->mlp_partial.release(); c->mlp_norm.release(); c->mlp_grad.release(); c->pred_conf.release(); c->pred_len.release(); c->mlp_loss.release(); c->mlp_idx.release(); c->mlp_ycount.release(); c->pred_count.release(); c->mlp_ylen.release(); c->cub_tmp.release(); c->out_tmp.release();
+  c->p_sen.release(); c->table_coarse.release(); c->walk_claim.release(); c->pr_count.release(); c->pr_off.release(); c->pr_rec.release(); c->pr_cstate.release(); c->pr_jump.release(); c->pr_cfirst.release(); c->p_negs.release(); c->sim.release(); c->bud_walks.release(); c->bud_len_sum.release(); c->bud_first_len.release(); c->bud_stop_round.release(); c->feat.release(); c->mlp_params.release(); c->mlp_m1.release(); c->mlp_m2.release(); c->mlp_partial.release(); c->mlp_norm.release(); c->mlp_grad.release(); c->pred_conf.release(); c->pred_len.release(); c->mlp_loss.release(); c->mlp_idx.release(); c->mlp_ycount.release(); c->pred_count.release(); c->mlp_ylen.release(); c->cub_tmp.release(); c->out_tmp.release();
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
   if (c->tm0) cudaEventDestroy(c->tm0);
@@ -855,6 +856,13 @@ extern "C" felog_status felog_init_model(felog_ctx *c) {
   CK(cudaMemcpy(c->id2offset.p, c->h_id2offset.data(), 4 * (size_t)V, cudaMemcpyHostToDevice), "init_model");
   CK(c->table.ensure(kTableSize), "init_model: unigram table");
   CK(cudaMemcpy(c->table.p, table.data(), 4 * (size_t)kTableSize, cudaMemcpyHostToDevice), "init_model");
+  {
+    const uint64_t nb = ((uint64_t)kTableSize + 63) >> kCoarseShift;
+    CK(c->table_coarse.ensure(nb), "init_model: unigram buckets");
+    k_unigram_coarse<<<grid_for(c, nb, 256), 256, 0, c->stream>>>(c->table.p, kTableSize, c->table_coarse.p);
+    c->launches++;
+    CK(cudaGetLastError(), "init_model: unigram buckets");
+  }
   c->use_thr = !thr.empty();
   CK(c->thr.ensure(std::max<size_t>(thr.size(), 1)), "init_model");
   if (c->use_thr) CK(cudaMemcpy(c->thr.p, thr.data(), 2 * thr.size(), cudaMemcpyHostToDevice), "init_model");
@@ -1057,6 +1065,7 @@ felog_status train_pairs(felog_ctx *c, SgArgs g, int blocks, int threads) {
   pa.cstate = c->pr_cstate.p;
   pa.cfirst = c->pr_cfirst.p;
   pa.reuse = c->o.reuse_neg ? 1 : 0;
+  pa.coarse = c->table_coarse.p;
   pa.negs = c->p_negs.p;
   pa.count = c->pr_count.p;
   pa.off = c->pr_off.p;

@@ -49,7 +49,31 @@ struct PairArgs {
   const unsigned long long *jump_a, *jump_c;  // the negative LCG advanced by K j steps, j < 2 window
   int reuse;             // -reuse-neg 1: full window, negatives from negs
   const int32_t *negs;   // plan negatives, K per sentence
+  const uint32_t *coarse;  // per 64-slot bucket of the unigram table (see k_unigram_coarse)
 };
+
+// The unigram table is nondecreasing (word2vec.cu:683-690), so a bucket of 64
+// slots holds one word iff its first and last slots agree.  coarse[k] is the
+// first slot's word, with the top bit set when the whole bucket is that word;
+// those slots are answered from this 6-MB array (L2-resident) instead of a
+// random read of the 400-MB table.
+constexpr int kCoarseShift = 6;
+constexpr uint32_t kCoarseUniform = 0x80000000u;
+
+__global__ void k_unigram_coarse(const int32_t *table, uint64_t table_size, uint32_t *coarse) {
+  const uint64_t nb = (table_size + (1u << kCoarseShift) - 1) >> kCoarseShift;
+  for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < nb; k += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t first = k << kCoarseShift;
+    const uint64_t last = min(first + (1u << kCoarseShift), table_size) - 1;
+    const int32_t w = table[first];
+    coarse[k] = (uint32_t)w | (table[last] == w ? kCoarseUniform : 0u);
+  }
+}
+
+__device__ __forceinline__ int32_t unigram_lookup(const int32_t *table, const uint32_t *coarse, uint64_t slot) {
+  const uint32_t c = __ldg(&coarse[slot >> kCoarseShift]);
+  return (c & kCoarseUniform) ? (int32_t)(c & ~kCoarseUniform) : __ldg(&table[slot]);
+}
 
 // number of valid contexts of the center at pos with window shrink b
 __device__ __forceinline__ int contexts_of(long long pos, long long sb, long long se, int window, int b) {
@@ -155,7 +179,7 @@ __global__ void __launch_bounds__(256) k_pair_emit(PairArgs a) {
 #pragma unroll
           for (int u = 0; u < U; u++) {
             nr[u] = nr[u] * 25214903917ULL + 11ULL;
-            t[u][q] = __ldg(&a.table[(nr[u] >> 16) % kUnigramSlots]);
+            t[u][q] = unigram_lookup(a.table, a.coarse, (nr[u] >> 16) % kUnigramSlots);
             if (t[u][q] == 0) t[u][q] = -2 - (int)fastmod(nr[u], a.fm_vocab1);  // fallback, resolved below
           }
       }

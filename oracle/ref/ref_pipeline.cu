@@ -104,17 +104,12 @@ int main(int argc, char **argv) {
   // the timed window opens at the hand-off of round warm-1, so it covers the
   // walks and the trainings of the timed rounds
   double t_start = now_s(), walk_s = 0, train_s = 0;
-  std::thread walker([&]() {
-    WalkerConfig<real_t, uint32_t> walker_conf(walkers);
-    auto ext = [&](Walker<uint32_t> &w, vertex_id_t) { return w.step >= 40 ? 0.0 : 1.0; };
-    TransitionConfig<real_t, uint32_t> tr(ext);
-    WalkConfig wc;
-    wc.set_output_file("bench");
-    graph.random_walk(&walker_conf, &tr, &wc);
-  });
-
   uint64_t tokens = 0, walk_tokens = 0, words = 0;
   double last_got = t_start;
+  double t_end = 0;
+  // trainer thread (felog.cpp runs train_corpus_cuda beside the walk, which
+  // stays on the main thread)
+  std::thread trainer([&]() {
   for (int r = 0; r < total_rounds; r++) {
     corpus_t corpus;
     {
@@ -154,8 +149,17 @@ int main(int argc, char **argv) {
     last_got = got;
     (void)t1;
   }
-  double t_end = now_s();
-  walker.join();
+  t_end = now_s();
+  });
+  {
+    WalkerConfig<real_t, uint32_t> walker_conf(walkers);
+    auto ext = [&](Walker<uint32_t> &w, vertex_id_t) { return w.step >= 40 ? 0.0 : 1.0; };
+    TransitionConfig<real_t, uint32_t> tr(ext);
+    WalkConfig wc;
+    wc.set_output_file("bench");
+    graph.random_walk(&walker_conf, &tr, &wc);
+  }
+  trainer.join();
   graph.out_queue.closeQueue();
   printf("{\"tokens\": %llu, \"seconds\": %.6f, \"walk_tokens\": %llu, \"walk_seconds\": %.6f, "
          "\"train_words\": %llu, \"train_seconds\": %.6f, \"threads\": %d, \"walkers\": %u}\n",
