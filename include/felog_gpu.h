@@ -218,6 +218,8 @@ felog_status felog_set_corpus(felog_ctx *ctx, const uint32_t *tokens, const uint
 felog_status felog_get_visit_freq(felog_ctx *ctx, uint64_t *freq);
 
 /* ---- trainer ---- */
+/* Vocabulary, unigram table and InitNet rows (word2vec.cu:834-902); also starts a new
+ * training run: stop flags, visit counts and the budget records are cleared. */
 felog_status felog_init_model(felog_ctx *ctx);
 felog_status felog_vocab_info(felog_ctx *ctx, uint64_t *vocab_size, uint64_t *train_words);
 felog_status felog_get_vocab(felog_ctx *ctx, uint32_t *vocab_vertex, uint32_t *id2offset);

@@ -888,6 +888,18 @@ extern "C" felog_status felog_init_model(felog_ctx *c) {
   CK(cudaGetLastError(), "init_model");
   CK(c->sim.ensure(V), "init_model");
   CK(cudaMemsetAsync(c->sim.p, 0, 4 * (size_t)V, c->stream), "init_model");
+  // a new training run: no stopped walkers, no visits, no budget history
+  CK(cudaMemsetAsync(c->stop.p, 0, V, c->stream), "init_model");
+  CK(cudaMemsetAsync(c->visit_freq.p, 0, sizeof(unsigned int) * (size_t)V, c->stream), "init_model");
+  c->words_sum_cum = 0;
+  c->have_last_eva = false;
+  c->pred_ready = false;
+  if (c->bud_walks.p) {
+    CK(cudaMemsetAsync(c->bud_walks.p, 0, 4 * (size_t)V, c->stream), "init_model");
+    CK(cudaMemsetAsync(c->bud_len_sum.p, 0, 4 * (size_t)V, c->stream), "init_model");
+    CK(cudaMemsetAsync(c->bud_first_len.p, 0, 4 * (size_t)V, c->stream), "init_model");
+    CK(cudaMemsetAsync(c->bud_stop_round.p, 0xFF, (size_t)V, c->stream), "init_model");
+  }
   CK(cudaStreamSynchronize(c->stream), "init_model");
   c->model_ready = true;
   return FELOG_OK;
