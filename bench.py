@@ -50,13 +50,26 @@ CONFIGS = {
     "prof": dict(workload="profiling case, seed-1 R-MAT 524,288 vertex ids / 8M undirected edges, 5% held out",
                  seed=1, v_target=524288, e_target=8_000_000, abcd=(0.57, 0.19, 0.19, 0.05), lognormal=False,
                  holdout=0.05),
+    "c4": dict(workload="plain FP32, seed-2 R-MAT (.6/.15/.15/.1) 3,072,441 vertex ids / 117M undirected edges, "
+                        "lognormal(0, 1) weights, 5% held out",
+               seed=2, v_target=3072441, e_target=117_000_000, abcd=(0.6, 0.15, 0.15, 0.1), lognormal=True,
+               holdout=0.05),
     "c1": dict(workload="plain FP32, seed-0 R-MAT 16,384 vertex ids / 131,072 undirected edges, 10% held out",
                seed=0, v_target=16384, e_target=131072, abcd=(0.57, 0.19, 0.19, 0.05), lognormal=False,
                holdout=0.10),
 }
 TRAIN = dict(min_length=20, min_rounds=2, size=128, window=10, negative=5, sample=1e-3, cbow=0, reuse_neg=0,
              min_count=0)
-FORMS = {"plain-fp32": dict(precision=0, budget_mode=0), "learned-bf16": dict(precision=1, budget_mode=1)}
+FORMS = {
+    # the reference's arithmetic, criterion and per-pair negatives
+    "plain-fp32": dict(precision=0, budget_mode=0, reuse_neg=0),
+    # BF16 tables + learned budget, per-pair negatives
+    "learned-bf16": dict(precision=1, budget_mode=1, reuse_neg=0),
+    # BF16 tables + learned budget, -reuse-neg 2 center tiles (shared negatives per sentence)
+    "learned-bf16-tile": dict(precision=1, budget_mode=1, reuse_neg=2),
+    # FP32 tables + learned budget + center tiles
+    "learned-fp32-tile": dict(precision=0, budget_mode=1, reuse_neg=2),
+}
 BUDGET_MODEL = os.path.join(ROOT, "info-centric_ge_b200", "felog_b200", "budget_mlp_c4.npy")
 METRIC = "walk+SGNS corpus tokens/s (walk steps/s and SGNS words/s reported alongside)"
 WALK_BYTES_PER_STEP = 68      # 2 random 32-B sectors + 4-B token write
@@ -179,6 +192,7 @@ def run_round(f, r, min_rounds, counters):
     counters["tokens"] += ws["n_tokens"]
     counters["words"] += ts["words"]
     counters["pairs"] += ts["pairs"]
+    counters["kept"] += ts["kept_words"]
     counters["walk_ms"] += ws["ms"]
     counters["train_ms"] += ts["ms_train"]
     counters["plan_ms"] += ts["ms_plan"]
@@ -224,7 +238,7 @@ def cpu_baseline(g, cfg):
 
 def new_context(fb, g, form, device, seed, model):
     V = g["v_num"]
-    f = fb.Felog(v_num=V, device=device, seed=seed, **FORMS[form], **TRAIN)
+    f = fb.Felog(v_num=V, device=device, seed=seed, **{**TRAIN, **FORMS[form]})
     f.load_graph(g["edges"], V)
     f.init_model()
     if FORMS[form]["budget_mode"] == 1:
@@ -257,7 +271,7 @@ def compare_forms(fb, g, device, model):
     seed; job time is the device time of the second of two runs in one context
     (the first one pays for allocations)."""
     out = {}
-    for form in ("plain-fp32", "learned-bf16"):
+    for form in ("plain-fp32", "learned-bf16", "learned-bf16-tile", "learned-fp32-tile"):
         f = new_context(fb, g, form, device, 77, model)
         f.run()         # untimed first run: device allocations and first-use module loading
         f.init_model()  # the timed run starts over from InitNet with the same walk seed
@@ -269,9 +283,11 @@ def compare_forms(fb, g, device, model):
                      "tokens_per_s": rs["walk_tokens"] / (rs["total_ms"] * 1e-3)}
         out[form]["auc"], out[form]["auc_centered"] = link_auc(f, g)
         f.close()
-    p, l = out["plain-fp32"], out["learned-bf16"]
-    out["end_to_end_speedup"] = p["job_ms"] / l["job_ms"]
-    out["auc_delta"] = l["auc"] - p["auc"]
+    p = out["plain-fp32"]
+    for form in ("learned-bf16", "learned-bf16-tile", "learned-fp32-tile"):
+        out[form]["end_to_end_speedup_vs_plain_fp32"] = p["job_ms"] / out[form]["job_ms"]
+        out[form]["auc_delta_vs_plain_fp32"] = out[form]["auc"] - p["auc"]
+        out[form]["auc_centered_delta_vs_plain_fp32"] = out[form]["auc_centered"] - p["auc_centered"]
     return out
 
 
@@ -286,7 +302,7 @@ def bench_mine(args):
     model = np.load(args.budget_model) if FORMS[form]["budget_mode"] or not args.no_forms else None
     f = new_context(fb, g, form, local, 1000 + rank, model)
     min_r = TRAIN["min_rounds"]
-    warm = {k: 0.0 for k in ("tokens", "words", "pairs", "walk_ms", "train_ms", "plan_ms", "budget_ms")}
+    warm = {k: 0.0 for k in ("tokens", "words", "pairs", "kept", "walk_ms", "train_ms", "plan_ms", "budget_ms")}
     for r in range(args.warmup):
         run_round(f, r, min_r, warm)
     log(f"warmup done: {warm}")
@@ -328,7 +344,15 @@ def bench_mine(args):
     e2e_value = sum_over_ranks(pg, e2e["tokens"]) / (e2e_ms * 1e-3)
     peak, peak_kind = measured_peaks()
     # dominant kernel: the skip-gram pass
-    sg_achieved = cnt["pairs"] * SGNS_BYTES_PER_PAIR[prec] / (cnt["train_ms"] * 1e-3) / 1e9
+    row_bytes = SGNS_BYTES_PER_PAIR[prec] // 14
+    if FORMS[form]["reuse_neg"] == 2:
+        # center tiles: per center its contexts and the K + 1 targets, each read and written once
+        sg_bytes = 2 * row_bytes * (cnt["pairs"] + (TRAIN["negative"] + 1) * cnt["kept"])
+        sg_kernel = f"k_sgns_reuse_tile<128, 5, Rows{prec.upper()}>"
+    else:
+        sg_bytes = cnt["pairs"] * SGNS_BYTES_PER_PAIR[prec]
+        sg_kernel = f"k_sgns_train_pairs<128, 5, Rows{prec.upper()}>"
+    sg_achieved = sg_bytes / (cnt["train_ms"] * 1e-3) / 1e9
     walk_achieved = cnt["tokens"] * WALK_BYTES_PER_STEP / (cnt["walk_ms"] * 1e-3) / 1e9
     out = {
         "metric": METRIC,
@@ -347,7 +371,7 @@ def bench_mine(args):
         "config": {"workload": cfg["workload"].replace("plain FP32", form), "form": form,
                    "v_num": V, "train_edges": int(len(g["edges"])),
                    "dim": 128, "window": 10, "negative": 5, "sample": 1e-3, "min_L": 20, "min_R": 2,
-                   "skip_gram": True, "reuse_neg": 0, "precision": prec,
+                   "skip_gram": True, "reuse_neg": FORMS[form]["reuse_neg"], "precision": prec,
                    "l2": "inputs larger than L2 (CSR + tables > 126 MB)",
                    "parallelism": f"replicas x{world}"},
         "walk_steps_per_s": cnt["tokens"] / (cnt["walk_ms"] * 1e-3),
@@ -355,7 +379,7 @@ def bench_mine(args):
         "phase_ms_per_step": {k: cnt[k] / args.steps for k in ("walk_ms", "plan_ms", "train_ms", "budget_ms")},
         "tokens_per_step": cnt["tokens"] / args.steps,
         "pairs_per_step": cnt["pairs"] / args.steps,
-        "roofline": {"kernel": f"k_sgns_skipgram<128, 5, Rows{prec.upper()}>", "bound": "hbm", "achieved": sg_achieved, "peak": peak,
+        "roofline": {"kernel": sg_kernel, "bound": "hbm", "achieved": sg_achieved, "peak": peak,
                      "unit": "GB/s", "frac": sg_achieved / peak, "traffic": None,
                      "peak_source": peak_kind,
                      "walk_kernel": {"achieved": walk_achieved, "frac": walk_achieved / peak,

@@ -1147,7 +1147,9 @@ extern "C" felog_status felog_train_round(felog_ctx *c, uint32_t round, float al
   if (!c->corpus_ready) return fail(c, FELOG_NOT_READY, "no corpus");
   // -reuse-neg applies to skip-gram only; with -cbow 1 the CBOW kernel runs (word2vec.cu:1255-1258)
   if (c->o.reuse_neg && !c->o.cbow && (c->o.size < 64 || (c->o.negative != 5 && c->o.negative != 7)))
-    return fail(c, FELOG_INVALID_ARG, "-reuse-neg 1 runs skip-gram with -negative 5 or 7 and -size >= 64");
+    return fail(c, FELOG_INVALID_ARG, "-reuse-neg runs skip-gram with -negative 5 or 7 and -size >= 64");
+  if (c->o.reuse_neg < 0 || c->o.reuse_neg > 2)
+    return fail(c, FELOG_INVALID_ARG, "-reuse-neg %d: 0, 1 (pair order) or 2 (center tiles)", c->o.reuse_neg);
   CK(cudaSetDevice(c->device), "train_round");
   if (alpha < 0) alpha = schedule_alpha(c, round);
   float ms_plan = 0, ms_train = 0;
@@ -1192,7 +1194,25 @@ extern "C" felog_status felog_train_round(felog_ctx *c, uint32_t round, float al
   const int blocks = c->o.deterministic ? 1 : c->sm_count * 8;
   const int threads = c->o.deterministic ? 32 : 256;
   CK(cudaEventRecord(c->ev0, c->stream), "train_round");
-  if (!c->o.cbow && c->o.size >= 64 && (c->o.negative == 5 || c->o.negative == 7)) {
+  if (!c->o.cbow && c->o.reuse_neg == 2) {
+    // center tiles over the plan negatives (k_sgns_reuse_tile)
+    const bool bf = c->o.precision == FELOG_BF16;
+#define FELOG_RT(D, K)                                                                      \
+  do {                                                                                      \
+    if (bf) k_sgns_reuse_tile<D, K, RowsBF16><<<blocks, threads, 0, c->stream>>>(g);       \
+    else k_sgns_reuse_tile<D, K, RowsF32><<<blocks, threads, 0, c->stream>>>(g);           \
+  } while (0)
+    const int K = c->o.negative, D = c->o.size;
+    if (K == 5 && D == 64) FELOG_RT(64, 5);
+    else if (K == 5 && D == 128) FELOG_RT(128, 5);
+    else if (K == 5 && D == 256) FELOG_RT(256, 5);
+    else if (K == 7 && D == 64) FELOG_RT(64, 7);
+    else if (K == 7 && D == 128) FELOG_RT(128, 7);
+    else FELOG_RT(256, 7);
+#undef FELOG_RT
+    c->launches++;
+    CK(cudaGetLastError(), "train_round: launch");
+  } else if (!c->o.cbow && c->o.size >= 64 && (c->o.negative == 5 || c->o.negative == 7)) {
     s = train_pairs(c, g, blocks, threads);
     if (s != FELOG_OK) return s;
   } else {

@@ -486,4 +486,103 @@ __global__ void __launch_bounds__(256, DIM >= 256 ? 2 : 4)
   if (lane == 0 && my_pairs) atomicAdd(a.pairs, my_pairs);
 }
 
+// -reuse-neg 2: __sgNegReuse's work (word2vec.cu:368-440: full window, the
+// sentence's K plan negatives) as one tile per center.  The K + 1 target rows
+// (the center word as positive, the negatives not equal to it) are read once
+// at the center; every context in window order is read fresh, scored against
+// them, and updated at once (syn0[c] += sum_j g_j y_j); the targets' updates
+// sum over the center's contexts and are applied once at the end of the
+// center (a negative that occurs twice gets the sum of both).  Per center this
+// reads and writes n + K + 1 rows instead of 2 (K + 1) n for the pair-by-pair
+// order, n being the number of contexts.
+template <int DIM, int NK, class P>
+__global__ void __launch_bounds__(256, 3) k_sgns_reuse_tile(SgArgs a) {
+  static_assert(DIM >= 64, "two or more values per lane");
+  constexpr int H = DIM / 64;
+  constexpr int NT = NK + 1;
+  static_assert(NT <= 8, "up to 8 targets");
+  __shared__ float s_exp[1000];
+  load_exp(a, s_exp);
+  const int lane = lane_id();
+  LaneRows<DIM, P> rows;
+  rows.init(a);
+  unsigned long long my_pairs = 0;
+  unsigned long long s;
+  while (claim_sentence(a, s)) {
+    const long long sb = (long long)a.sent_start[s], se = (long long)a.sent_start[s + 1];
+    int neg[NK];
+#pragma unroll
+    for (int q = 0; q < NK; q++) neg[q] = __ldg(&a.negs[s * (uint64_t)NK + q]);
+    for (long long pos = sb; pos < se; pos++) {
+      const int word = __ldg(&a.sen[pos]);
+      long long c0 = pos - a.window, c1 = pos + a.window;
+      if (c0 < sb) c0 = sb;
+      if (c1 > se - 1) c1 = se - 1;
+      if (c1 - c0 < 1) continue;  // no context
+      int tg[NT];
+      tg[0] = word;
+#pragma unroll
+      for (int q = 0; q < NK; q++) tg[q + 1] = neg[q] == word ? -1 : neg[q];
+      float2 y[NT][H], dy[NT][H];
+#pragma unroll
+      for (int q = 0; q < NT; q++) {
+#pragma unroll
+        for (int k = 0; k < H; k++) {
+          y[q][k] = make_float2(0.0f, 0.0f);
+          dy[q][k] = make_float2(0.0f, 0.0f);
+        }
+        if (tg[q] >= 0) rows.template load<1>((uint32_t)tg[q], y[q]);
+      }
+      const uint32_t center = (uint32_t)(pos - sb);
+      const uint32_t key = P::kBF16 ? lane_key(a.sr_seed, s, center, lane) : 0u;
+      const int tq = butterfly_target(lane);
+      uint32_t vmask = 0;
+#pragma unroll
+      for (int q = 0; q < NT; q++) vmask |= (tg[q] >= 0 ? 1u : 0u) << q;
+      const bool lane_scores = tq < NT && ((vmask >> tq) & 1u);
+      for (long long c = c0; c <= c1; c++) {
+        if (c == pos) continue;
+        const uint32_t l1 = (uint32_t)__ldg(&a.sen[c]);
+        float2 x[H];
+        rows.template load<0>(l1, x);
+        const float z = multi_dot2<H, NT>(x, y);
+        const float gv = lane_scores ? sg_grad(z, tq == 0 ? 1 : 0, s_exp, a.alpha) : 0.0f;
+        float2 neu[H];
+#pragma unroll
+        for (int k = 0; k < H; k++) neu[k] = make_float2(0.0f, 0.0f);
+#pragma unroll
+        for (int q = 0; q < NT; q++) {
+          const float g = __shfl_sync(0xffffffffu, gv, butterfly_lane(q));
+          if (tg[q] < 0) continue;
+          const float2 g2 = make_float2(g, g);
+#pragma unroll
+          for (int k = 0; k < H; k++) {
+            neu[k] = __ffma2_rn(g2, y[q][k], neu[k]);
+            dy[q][k] = __ffma2_rn(g2, x[k], dy[q][k]);
+          }
+        }
+        rows.template update<0>(l1, neu, x, slot_stream(key, kSlotCtx + (uint32_t)(c - pos + a.window)));
+        my_pairs++;
+      }
+      // targets: a repeated negative adds its sum into the first occurrence
+#pragma unroll
+      for (int q = 2; q < NT; q++) {
+        bool merged = false;
+#pragma unroll
+        for (int r = 1; r < q; r++) {
+          const bool hit = !merged && tg[q] >= 0 && tg[r] == tg[q];
+#pragma unroll
+          for (int k = 0; k < H; k++) dy[r][k] = hit ? __fadd2_rn(dy[r][k], dy[q][k]) : dy[r][k];
+          merged |= hit;
+        }
+        if (merged) tg[q] = -2;  // applied through its first occurrence
+      }
+#pragma unroll
+      for (int q = 0; q < NT; q++)
+        if (tg[q] >= 0) rows.template update<1>((uint32_t)tg[q], dy[q], y[q], slot_stream(key, (uint32_t)q));
+    }
+  }
+  if (lane == 0 && my_pairs) atomicAdd(a.pairs, my_pairs);
+}
+
 }  // namespace felog

@@ -709,6 +709,73 @@ void orc_negreuse_bf16(float *syn0, uint16_t *syn0_bf, float *syn1, uint16_t *sy
                n_sentences, window, dim, negative, alpha, negs);
 }
 
+/* -reuse-neg 2 (this project's option): __sgNegReuse's work (full window, the
+ * sentence's K plan negatives) as one tile per center.  Per center: the K + 1
+ * target rows (center word as positive, negatives not equal to it) are read
+ * once; every context in window order is read fresh, scored against them with
+ * the tree dot, and updated at once (x += sum_j g_j y_j, j in order); the
+ * targets' updates dy_j = sum over contexts of g_j x (context order) are
+ * applied at the end of the center, a negative that occurs twice adding its
+ * dy into its first occurrence.  Rows in the mixed storage form (n_hot =
+ * vocab_size: all FP32); rounding streams as orc_skipgram_bf16 with the
+ * center's index in the sentence as the pair index, slot j for targets and
+ * 256 + window position for contexts. */
+void orc_negreuse_tile(float *syn0, uint16_t *syn0_bf, float *syn1, uint16_t *syn1_bf, long long n_hot,
+                       uint32_t sr_seed, const float *exp_table, const int32_t *sen, const uint64_t *sent_start,
+                       uint64_t first_sentence, uint64_t n_sentences, const int32_t *negs, int window, int dim,
+                       int negative, float alpha) {
+  mixed_rows m0 = {syn0, syn0_bf, n_hot, dim}, m1 = {syn1, syn1_bf, n_hot, dim};
+  float x[512], neu1e[512];
+  float y[16][512], dy[16][512];
+  int tg[16];
+  for (uint64_t blk = 0; blk < n_sentences; blk++) {
+    uint64_t s = first_sentence + blk;
+    long long ss = (long long)sent_start[s], se = (long long)sent_start[s + 1];
+    const int32_t *neg = negs + s * (uint64_t)negative;
+    for (long long pos = ss; pos < se; pos++) {
+      int word = sen[pos];
+      long long c0 = pos - window < ss ? ss : pos - window;
+      long long c1 = pos + window > se - 1 ? se - 1 : pos + window;
+      if (c1 - c0 < 1) continue;
+      int nt = negative + 1;
+      tg[0] = word;
+      for (int q = 0; q < negative; q++) tg[q + 1] = neg[q] == word ? -1 : neg[q];
+      for (int q = 0; q < nt; q++) {
+        for (int t = 0; t < dim; t++) dy[q][t] = 0;
+        if (tg[q] >= 0) mr_get(&m1, tg[q], y[q]);
+      }
+      uint32_t center = (uint32_t)(pos - ss);
+      for (long long c = c0; c <= c1; c++) {
+        if (c == pos) continue;
+        int l1 = sen[c];
+        mr_get(&m0, l1, x);
+        for (int t = 0; t < dim; t++) neu1e[t] = 0;
+        for (int q = 0; q < nt; q++) {
+          if (tg[q] < 0) continue;
+          float f = sg_dot(x, y[q], dim);
+          float g = sg_gradient(f, q == 0 ? 1 : 0, exp_table, alpha);
+          for (int t = 0; t < dim; t++) {
+            neu1e[t] = fmaf(g, y[q][t], neu1e[t]);
+            dy[q][t] = fmaf(g, x[t], dy[q][t]);
+          }
+        }
+        mr_add(&m0, l1, x, neu1e, sr_seed, s, center, 256u + (uint32_t)(c - pos + window));
+      }
+      for (int q = 2; q < nt; q++) {
+        if (tg[q] < 0) continue;
+        for (int r = 1; r < q; r++)
+          if (tg[r] == tg[q]) {
+            for (int t = 0; t < dim; t++) dy[r][t] = dy[r][t] + dy[q][t];
+            tg[q] = -2;
+            break;
+          }
+      }
+      for (int q = 0; q < nt; q++)
+        if (tg[q] >= 0) mr_add(&m1, tg[q], y[q], dy[q], sr_seed, s, center, (uint32_t)q);
+    }
+  }
+}
+
 void orc_cbow_bf16(float *syn0, uint16_t *syn0_bf, float *syn1, uint16_t *syn1_bf, long long n_hot,
                    uint32_t sr_seed, const float *exp_table, const int32_t *table, int64_t table_size,
                    long long vocab_size, const int32_t *sen, const uint64_t *sent_start, uint64_t first_sentence,

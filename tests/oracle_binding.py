@@ -86,6 +86,9 @@ def lib():
                                         ctypes.c_int64, ctypes.c_longlong, i32p, u64p, ctypes.c_uint64,
                                         ctypes.c_uint64, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float]
         L.orc_cbow_bf16.argtypes = L.orc_skipgram_bf16.argtypes
+        L.orc_negreuse_tile.argtypes = [f32p, u16p, f32p, u16p, ctypes.c_longlong, ctypes.c_uint32, f32p, i32p, u64p,
+                                        ctypes.c_uint64, ctypes.c_uint64, i32p, ctypes.c_int, ctypes.c_int,
+                                        ctypes.c_int, ctypes.c_float]
         L.orc_negreuse_bf16.argtypes = [f32p, u16p, f32p, u16p, ctypes.c_longlong, ctypes.c_uint32, f32p, i32p, u64p,
                                         ctypes.c_uint64, ctypes.c_uint64, i32p, ctypes.c_int, ctypes.c_int,
                                         ctypes.c_int, ctypes.c_float]
@@ -290,6 +293,14 @@ def mlp_loss_grad(params, X, count, length):
 
 def negreuse_bf16(m0, m1, sr_seed, exp_tab, sen, sent_start, first, n, negs, window, dim, negative, alpha):
     lib().orc_negreuse_bf16(ptr(m0.f32, f32p), ptr(m0.bf, u16p), ptr(m1.f32, f32p), ptr(m1.bf, u16p), m0.n_hot,
+                            sr_seed, ptr(exp_tab, f32p), ptr(np.ascontiguousarray(sen, np.int32), i32p),
+                            ptr(np.ascontiguousarray(sent_start, np.uint64), u64p), first, n,
+                            ptr(np.ascontiguousarray(negs, np.int32), i32p), window, dim, negative, alpha)
+
+
+def negreuse_tile(m0, m1, sr_seed, exp_tab, sen, sent_start, first, n, negs, window, dim, negative, alpha):
+    """-reuse-neg 2 center tiles on MixedRows (n_hot = vocab size for the FP32 form)."""
+    lib().orc_negreuse_tile(ptr(m0.f32, f32p), ptr(m0.bf, u16p), ptr(m1.f32, f32p), ptr(m1.bf, u16p), m0.n_hot,
                             sr_seed, ptr(exp_tab, f32p), ptr(np.ascontiguousarray(sen, np.int32), i32p),
                             ptr(np.ascontiguousarray(sent_start, np.uint64), u64p), first, n,
                             ptr(np.ascontiguousarray(negs, np.int32), i32p), window, dim, negative, alpha)

@@ -105,6 +105,36 @@ def test_bf16_reuse_neg_deterministic_matches_oracle(dim):
     assert exact == (1.0, 1.0), f"fraction bit-exact syn0/syn1: {exact}"
 
 
+@pytest.mark.parametrize("precision,dim,negative", [(0, 128, 5), (1, 128, 5), (0, 64, 7), (1, 256, 5)])
+def test_reuse_tile_deterministic_matches_oracle(precision, dim, negative):
+    """-reuse-neg 2 (one tile per center) in the one-warp mode, FP32 and BF16
+    forms, against the oracle's restatement."""
+    e, V = graph4096()
+    f = fb.Felog(v_num=V, size=dim, window=5, negative=negative, sample=1e-3, cbow=0, reuse_neg=2, min_count=0,
+                 precision=precision, deterministic=1, seed=SEED)
+    f.load_graph(e, V)
+    f.init_model()
+    _, _, vs, _ = f.vocab()
+    nh = n_hot(vs) if precision else vs
+    o0, o1 = ob.init_net(vs, dim)
+    m0, m1 = ob.MixedRows(o0, vs, dim, nh), ob.MixedRows(o1, vs, dim, nh)
+    tok, off = walk_corpus(V, e, 300, seed=6)
+    f.set_corpus(tok, off)
+    f.train_round(0, alpha=0.025)
+    c = ob.OracleCsr(e, V)
+    vv, vcn, id2, _, tw = ob.vocab(c.deg, 0)
+    thr, used = ob.subsample_thresholds(vcn, 1e-3, tw)
+    table = ob.unigram_table(vcn)
+    pl = ob.plan_batches(tok, off, id2, thr, used, table, vs, negative)
+    bf = pl["batch_first"]
+    for b in range(len(bf) - 1):
+        ob.negreuse_tile(m0, m1, ob.round_sr_seed(SEED, 0), ob.exp_table(), pl["sen"], pl["sent_start"], int(bf[b]),
+                         int(bf[b + 1] - bf[b]), pl["negs"], 5, dim, negative, 0.025)
+    g0, g1 = f.embeddings()
+    exact = np.mean(g0 == m0.full()), np.mean(g1 == m1.full())
+    assert exact == (1.0, 1.0), f"fraction bit-exact syn0/syn1: {exact}"
+
+
 def link_auc(s0, id2, vs, dim, g):
     e0 = s0.reshape(vs, dim)[id2]
     n0 = e0 / np.maximum(np.linalg.norm(e0, axis=1, keepdims=True), 1e-30)
