@@ -78,7 +78,8 @@ typedef struct felog_opts {
   int32_t negative;         /* -negative (1..15) */
   int32_t hs;               /* -hs (must be 0) */
   int32_t cbow;             /* -cbow */
-  int32_t reuse_neg;        /* -reuse-neg: 1 the reference's pair order; 2 (B200 option) one tile per center */
+  int32_t reuse_neg;        /* -reuse-neg: 1 the reference's pair order; B200 options: 2 one tile per center,
+                               3 center tiles scored on the tensor cores (BF16 form) */
   int32_t iter;             /* -iter (parsed, unused like the reference) */
   int32_t min_count;        /* -min-count */
   int32_t classes;          /* -classes (K-means output) */

@@ -1148,8 +1148,13 @@ extern "C" felog_status felog_train_round(felog_ctx *c, uint32_t round, float al
   // -reuse-neg applies to skip-gram only; with -cbow 1 the CBOW kernel runs (word2vec.cu:1255-1258)
   if (c->o.reuse_neg && !c->o.cbow && (c->o.size < 64 || (c->o.negative != 5 && c->o.negative != 7)))
     return fail(c, FELOG_INVALID_ARG, "-reuse-neg runs skip-gram with -negative 5 or 7 and -size >= 64");
-  if (c->o.reuse_neg < 0 || c->o.reuse_neg > 2)
-    return fail(c, FELOG_INVALID_ARG, "-reuse-neg %d: 0, 1 (pair order) or 2 (center tiles)", c->o.reuse_neg);
+  if (c->o.reuse_neg < 0 || c->o.reuse_neg > 3)
+    return fail(c, FELOG_INVALID_ARG, "-reuse-neg %d: 0, 1 (pair order), 2 (center tiles) or 3 (tensor-core tiles)",
+                c->o.reuse_neg);
+  if (c->o.reuse_neg == 3 && !c->o.cbow &&
+      (c->o.precision != FELOG_BF16 || (c->o.size != 64 && c->o.size != 128) || 2 * c->o.window > kTileRows))
+    return fail(c, FELOG_INVALID_ARG, "-reuse-neg 3 needs the BF16 form, -size 64 or 128 and -window <= %d",
+                kTileRows / 2);
   CK(cudaSetDevice(c->device), "train_round");
   if (alpha < 0) alpha = schedule_alpha(c, round);
   float ms_plan = 0, ms_train = 0;
@@ -1194,7 +1199,18 @@ extern "C" felog_status felog_train_round(felog_ctx *c, uint32_t round, float al
   const int blocks = c->o.deterministic ? 1 : c->sm_count * 8;
   const int threads = c->o.deterministic ? 32 : 256;
   CK(cudaEventRecord(c->ev0, c->stream), "train_round");
-  if (!c->o.cbow && c->o.reuse_neg == 2) {
+  if (!c->o.cbow && c->o.reuse_neg == 3) {
+    // center tiles scored on the tensor cores (k_sgns_reuse_tile_tc)
+    const int tb = c->o.deterministic ? 1 : c->sm_count * 16;
+    const int tt = c->o.deterministic ? 32 : 32 * kTileWarps;
+    const int K = c->o.negative, D = c->o.size;
+    if (K == 5 && D == 64) k_sgns_reuse_tile_tc<64, 5><<<tb, tt, 0, c->stream>>>(g);
+    else if (K == 5 && D == 128) k_sgns_reuse_tile_tc<128, 5><<<tb, tt, 0, c->stream>>>(g);
+    else if (K == 7 && D == 64) k_sgns_reuse_tile_tc<64, 7><<<tb, tt, 0, c->stream>>>(g);
+    else k_sgns_reuse_tile_tc<128, 7><<<tb, tt, 0, c->stream>>>(g);
+    c->launches++;
+    CK(cudaGetLastError(), "train_round: launch");
+  } else if (!c->o.cbow && c->o.reuse_neg == 2) {
     // center tiles over the plan negatives (k_sgns_reuse_tile)
     const bool bf = c->o.precision == FELOG_BF16;
 #define FELOG_RT(D, K)                                                                      \

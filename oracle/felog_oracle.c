@@ -776,6 +776,106 @@ void orc_negreuse_tile(float *syn0, uint16_t *syn0_bf, float *syn1, uint16_t *sy
   }
 }
 
+/* -reuse-neg 3 (this project's option, BF16 form): the center tile scored on
+ * tensor cores.  Per center all contexts (window order) and targets are read at
+ * the start of the center; scores are dots of their round-to-nearest BF16
+ * copies (the tensor core accumulates in FP32 in an unspecified order; here the
+ * sum is FP64, rounded to FP32, so a test compares within a tolerance).
+ * Rows of G belonging to a repeated context word are added into its first
+ * occurrence (column by column, in window order); then, per context in order,
+ * neu = sum_j G_cj y_j (y exact) and dy_j += G_cj xb_c (xb the BF16 copy); the
+ * first occurrence of each context word is updated once; targets as in
+ * orc_negreuse_tile. */
+static float bf16_round_rn(float v) {
+  uint32_t b;
+  memcpy(&b, &v, 4);
+  b = (b + 0x7FFFu + ((b >> 16) & 1u)) & 0xFFFF0000u;
+  memcpy(&v, &b, 4);
+  return v;
+}
+
+void orc_negreuse_tile_tc(float *syn0, uint16_t *syn0_bf, float *syn1, uint16_t *syn1_bf, long long n_hot,
+                          uint32_t sr_seed, const float *exp_table, const int32_t *sen, const uint64_t *sent_start,
+                          uint64_t first_sentence, uint64_t n_sentences, const int32_t *negs, int window, int dim,
+                          int negative, float alpha) {
+  mixed_rows m0 = {syn0, syn0_bf, n_hot, dim}, m1 = {syn1, syn1_bf, n_hot, dim};
+  static float xb[64][512], y[16][512], yb[16][512], dy[16][512];
+  float neu1e[512], G[64][16];
+  int tg[16], cw[64], first[64];
+  long long cpos[64];
+  for (uint64_t blk = 0; blk < n_sentences; blk++) {
+    uint64_t s = first_sentence + blk;
+    long long ss = (long long)sent_start[s], se = (long long)sent_start[s + 1];
+    const int32_t *neg = negs + s * (uint64_t)negative;
+    for (long long pos = ss; pos < se; pos++) {
+      int word = sen[pos];
+      long long c0 = pos - window < ss ? ss : pos - window;
+      long long c1 = pos + window > se - 1 ? se - 1 : pos + window;
+      int n = (int)(c1 - c0);
+      if (n < 1) continue;
+      int nt = negative + 1;
+      tg[0] = word;
+      for (int q = 0; q < negative; q++) tg[q + 1] = neg[q] == word ? -1 : neg[q];
+      for (int q = 0; q < nt; q++) {
+        for (int t = 0; t < dim; t++) y[q][t] = 0, dy[q][t] = 0;
+        if (tg[q] >= 0) mr_get(&m1, tg[q], y[q]);
+        for (int t = 0; t < dim; t++) yb[q][t] = bf16_round_rn(y[q][t]);
+      }
+      for (int i = 0; i < n; i++) {
+        long long c = c0 + i;
+        if (c >= pos) c++;
+        cpos[i] = c;
+        cw[i] = sen[c];
+        mr_get(&m0, cw[i], xb[i]);
+        for (int t = 0; t < dim; t++) xb[i][t] = bf16_round_rn(xb[i][t]);
+        first[i] = i;
+        for (int j = 0; j < i; j++)
+          if (cw[j] == cw[i]) {
+            first[i] = j;
+            break;
+          }
+      }
+      for (int i = 0; i < n; i++)
+        for (int q = 0; q < nt; q++) {
+          G[i][q] = 0;
+          if (tg[q] < 0) continue;
+          double f = 0;
+          for (int t = 0; t < dim; t++) f += (double)xb[i][t] * (double)yb[q][t];
+          G[i][q] = sg_gradient((float)f, q == 0 ? 1 : 0, exp_table, alpha);
+        }
+      for (int q = 0; q < nt; q++)
+        for (int i = 1; i < n; i++)
+          if (first[i] != i) {
+            G[first[i]][q] = G[first[i]][q] + G[i][q];
+            G[i][q] = 0;
+          }
+      uint32_t center = (uint32_t)(pos - ss);
+      for (int i = 0; i < n; i++) {
+        for (int t = 0; t < dim; t++) neu1e[t] = 0;
+        for (int q = 0; q < nt; q++) {
+          float g = G[i][q];
+          for (int t = 0; t < dim; t++) {
+            neu1e[t] = fmaf(g, y[q][t], neu1e[t]);
+            dy[q][t] = fmaf(g, xb[i][t], dy[q][t]);
+          }
+        }
+        if (first[i] == i) mr_add(&m0, cw[i], xb[i], neu1e, sr_seed, s, center, 256u + (uint32_t)(cpos[i] - pos + window));
+      }
+      for (int q = 2; q < nt; q++) {
+        if (tg[q] < 0) continue;
+        for (int r = 1; r < q; r++)
+          if (tg[r] == tg[q]) {
+            for (int t = 0; t < dim; t++) dy[r][t] = dy[r][t] + dy[q][t];
+            tg[q] = -2;
+            break;
+          }
+      }
+      for (int q = 0; q < nt; q++)
+        if (tg[q] >= 0) mr_add(&m1, tg[q], y[q], dy[q], sr_seed, s, center, (uint32_t)q);
+    }
+  }
+}
+
 void orc_cbow_bf16(float *syn0, uint16_t *syn0_bf, float *syn1, uint16_t *syn1_bf, long long n_hot,
                    uint32_t sr_seed, const float *exp_table, const int32_t *table, int64_t table_size,
                    long long vocab_size, const int32_t *sen, const uint64_t *sent_start, uint64_t first_sentence,

@@ -89,6 +89,7 @@ def lib():
         L.orc_negreuse_tile.argtypes = [f32p, u16p, f32p, u16p, ctypes.c_longlong, ctypes.c_uint32, f32p, i32p, u64p,
                                         ctypes.c_uint64, ctypes.c_uint64, i32p, ctypes.c_int, ctypes.c_int,
                                         ctypes.c_int, ctypes.c_float]
+        L.orc_negreuse_tile_tc.argtypes = L.orc_negreuse_tile.argtypes
         L.orc_negreuse_bf16.argtypes = [f32p, u16p, f32p, u16p, ctypes.c_longlong, ctypes.c_uint32, f32p, i32p, u64p,
                                         ctypes.c_uint64, ctypes.c_uint64, i32p, ctypes.c_int, ctypes.c_int,
                                         ctypes.c_int, ctypes.c_float]
@@ -304,6 +305,14 @@ def negreuse_tile(m0, m1, sr_seed, exp_tab, sen, sent_start, first, n, negs, win
                             sr_seed, ptr(exp_tab, f32p), ptr(np.ascontiguousarray(sen, np.int32), i32p),
                             ptr(np.ascontiguousarray(sent_start, np.uint64), u64p), first, n,
                             ptr(np.ascontiguousarray(negs, np.int32), i32p), window, dim, negative, alpha)
+
+
+def negreuse_tile_tc(m0, m1, sr_seed, exp_tab, sen, sent_start, first, n, negs, window, dim, negative, alpha):
+    """-reuse-neg 3 (tensor-core center tiles) on MixedRows."""
+    lib().orc_negreuse_tile_tc(ptr(m0.f32, f32p), ptr(m0.bf, u16p), ptr(m1.f32, f32p), ptr(m1.bf, u16p), m0.n_hot,
+                               sr_seed, ptr(exp_tab, f32p), ptr(np.ascontiguousarray(sen, np.int32), i32p),
+                               ptr(np.ascontiguousarray(sent_start, np.uint64), u64p), first, n,
+                               ptr(np.ascontiguousarray(negs, np.int32), i32p), window, dim, negative, alpha)
 
 
 def negreuse_batch(syn0, syn1, exp_tab, sen, sent_start, first, n, negs, window, dim, negative, alpha):

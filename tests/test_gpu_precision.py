@@ -135,6 +135,46 @@ def test_reuse_tile_deterministic_matches_oracle(precision, dim, negative):
     assert exact == (1.0, 1.0), f"fraction bit-exact syn0/syn1: {exact}"
 
 
+@pytest.mark.parametrize("dim,negative", [(128, 5), (64, 7)])
+def test_reuse_tile_tensor_core_matches_oracle(dim, negative):
+    """-reuse-neg 3 (BF16 form, center tiles scored by mma.sync bf16) in the
+    one-warp mode against the oracle's restatement with FP64 dots of the same
+    BF16 operands.  The tensor core's FP32 accumulation order is unspecified,
+    so a score can differ in its last bits and flip a stochastic rounding that
+    later centers then read: the tables must agree bit for bit on >= 99% of the
+    values and within a few BF16 ulps (2^-5 relative, 1e-6 absolute) everywhere."""
+    e, V = graph4096()
+    f = fb.Felog(v_num=V, size=dim, window=5, negative=negative, sample=1e-3, cbow=0, reuse_neg=3, min_count=0,
+                 precision=1, deterministic=1, seed=SEED)
+    f.load_graph(e, V)
+    f.init_model()
+    _, _, vs, _ = f.vocab()
+    nh = n_hot(vs)
+    o0, o1 = ob.init_net(vs, dim)
+    m0, m1 = ob.MixedRows(o0, vs, dim, nh), ob.MixedRows(o1, vs, dim, nh)
+    tok, off = walk_corpus(V, e, 300, seed=6)
+    f.set_corpus(tok, off)
+    st = f.train_round(0, alpha=0.025)
+    assert st["pairs"] > 0
+    c = ob.OracleCsr(e, V)
+    vv, vcn, id2, _, tw = ob.vocab(c.deg, 0)
+    thr, used = ob.subsample_thresholds(vcn, 1e-3, tw)
+    table = ob.unigram_table(vcn)
+    pl = ob.plan_batches(tok, off, id2, thr, used, table, vs, negative)
+    bf = pl["batch_first"]
+    for b in range(len(bf) - 1):
+        ob.negreuse_tile_tc(m0, m1, ob.round_sr_seed(SEED, 0), ob.exp_table(), pl["sen"], pl["sent_start"],
+                            int(bf[b]), int(bf[b + 1] - bf[b]), pl["negs"], 5, dim, negative, 0.025)
+    g0, g1 = f.embeddings()
+    r0, r1 = m0.full(), m1.full()
+    for g, r in ((g0, r0), (g1, r1)):
+        exact = np.mean(g == r)
+        d = np.abs(g - r)
+        print(f"tensor-core tile vs oracle: exact {exact:.5f}, max abs diff {d.max():.3e}")
+        assert exact >= 0.99
+        assert np.all(d <= 2.0 ** -5 * np.abs(r) + 1e-6)
+
+
 def link_auc(s0, id2, vs, dim, g):
     e0 = s0.reshape(vs, dim)[id2]
     n0 = e0 / np.maximum(np.linalg.norm(e0, axis=1, keepdims=True), 1e-30)
