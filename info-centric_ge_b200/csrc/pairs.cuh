@@ -242,19 +242,14 @@ struct LaneRows {
     if constexpr (!P::kBF16) {
       load_f32(pf, r);
     } else {
-      const bool hot = row < n_hot;
-      const uint16_t *pb = b[W] + (size_t)row * DIM;
-      float2 fv[H];
-      uint32_t hv[H];
+      if (row < n_hot) {
+        load_f32(pf, r);
+      } else {
+        uint32_t hv[H];
+        load_b16(b[W] + (size_t)row * DIM, hv);
 #pragma unroll
-      for (int k = 0; k < H; k++) {
-        fv[k] = make_float2(0.0f, 0.0f);
-        hv[k] = 0u;
+        for (int k = 0; k < H; k++) r[k] = make_float2(bf16_lo(hv[k]), bf16_hi(hv[k]));
       }
-      if (hot) load_f32(pf, fv);
-      else load_b16(pb, hv);
-#pragma unroll
-      for (int k = 0; k < H; k++) r[k] = hot ? fv[k] : make_float2(bf16_lo(hv[k]), bf16_hi(hv[k]));
     }
   }
 

@@ -133,11 +133,11 @@ __host__ __device__ __forceinline__ uint32_t sr_hash(uint32_t x) {
 // Rounding streams.  One hash per (sentence, pair, lane) gives the lane's key;
 // the stream of row slot `slot` (target index d = 0..K for syn1 rows,
 // kSlotCtx (+ window position for CBOW) for syn0 rows) starts at
-// key + slot * 0x27D4EB2F and takes one LCG step per two values: the word
-// R = x ^ (x >> 16) of the new state x gives its low 16 bits to the lane's
-// value 2k and its high 16 bits to value 2k + 1.  Every value's 16 bits are
-// uniform, so each rounding is unbiased; the streams depend on (seed,
-// sentence, pair, slot, lane) only.
+// key + slot * 0x27D4EB2F and takes one LCG step per two values: the new
+// state x gives its low 16 bits to the lane's value 2k and its high 16 bits to
+// value 2k + 1.  The start is hashed and a stream runs at most four steps, so
+// every value's 16 bits are uniform and each rounding is unbiased; the streams
+// depend on (seed, sentence, pair, slot, lane) only.
 constexpr uint32_t kSlotCtx = 256;
 __host__ __device__ __forceinline__ uint32_t lane_key(uint32_t seed, uint64_t s, uint32_t pair, uint32_t lane) {
   return sr_hash(seed ^ ((uint32_t)s * 0x9E3779B1u + pair * 0x85EBCA77u + lane * 0xC2B2AE3Du));
@@ -147,7 +147,7 @@ __host__ __device__ __forceinline__ uint32_t slot_stream(uint32_t key, uint32_t 
 }
 __device__ __forceinline__ uint32_t sr_word(uint32_t &st) {
   st = st * 1664525u + 1013904223u;
-  return st ^ (st >> 16);
+  return st;
 }
 // Two FP32 values to packed BF16 by stochastic rounding in one instruction
 // (sm_100a cvt.rs): hi goes to the upper half with random bits r >> 16, lo to

@@ -558,9 +558,9 @@ void orc_cbow_batch(float *syn0, float *syn1, const float *exp_table, const int3
  * truncation.  The bits of one (pair, slot, lane) come from a keyed stream:
  *   key    = H(seed ^ ((u32)s * 0x9E3779B1 + pair * 0x85EBCA77 + lane * 0xC2B2AE3D))
  *   stream = key + slot * 0x27D4EB2F
- *   word k = x ^ (x >> 16) with x = (stream = stream * 1664525 + 1013904223),
- *            one per two values: its low 16 bits round the lane's value 2k,
- *            its high 16 bits value 2k + 1
+ *   word k = (stream = stream * 1664525 + 1013904223), one per two values:
+ *            its low 16 bits round the lane's value 2k, its high 16 bits
+ *            value 2k + 1
  * (s: sentence index in the plan; pair: index of the (center, context) pair in
  * the sentence, or of the center for CBOW)  * where H is a multiply / xor-shift mixer, slot = d (target index, 0 is the
  * positive) for syn1 rows and 256 (+ window position a for CBOW) for syn0
@@ -618,7 +618,7 @@ static void mr_add(const mixed_rows *m, long long row, const float *cur, const f
       int t = lane + 32 * j;
       if ((j & 1) == 0) {
         st = st * 1664525u + 1013904223u;
-        w = st ^ (st >> 16);
+        w = st;
       }
       b[t] = f_to_bf_sr(cur[t] + u[t], (j & 1) ? (w >> 16) : (w & 0xFFFFu));
     }

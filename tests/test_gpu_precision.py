@@ -198,10 +198,11 @@ def run_form(g, precision, seed=17):
 
 def test_bf16_auc_within_0005_of_fp32():
     """End-to-end embeddings of the BF16 form against the FP32 form on the same
-    graph and walk seed.  (After a fixed number of rounds two FP32 Hogwild runs
-    already differ by ~0.001 and the sequential FP32 order by ~0.005 on this
-    graph, so the bar is applied to the finished runs.)"""
-    g = fb.synth_graph(seed=3, v_target=16384, e_target=131072, holdout=0.1)
+    graph and walk seed, run to completion.  The graph has ~100 k held-out
+    pairs, so the AUC estimate itself has a standard error near 0.001; on a
+    16 k-vertex graph it is ~0.002 and the forms can also stop after a
+    different number of rounds, which makes a 0.005 bar a coin toss there."""
+    g = fb.synth_graph(seed=3, v_target=65536, e_target=1048576, holdout=0.1)
     s32, id2, vs, st32 = run_form(g, 0)
     s16, id2b, vsb, st16 = run_form(g, 1)
     assert np.isfinite(s16).all()
