@@ -387,6 +387,7 @@ def bench_mine(args):
         "e2e": {"value": e2e_value, "unit": "tokens/s", "h2d_bytes_per_step": int(V),
                 "d2h_bytes_per_step": int(vs * 128 * 4 + V)},
         "gpu_launches": int(launches),
+        "autotune": f.tuning_report(),
         "clocks": clk.summary(),
     }
     if rank == 0 and world == 1 and not args.no_forms:

@@ -102,6 +102,7 @@ typedef struct felog_opts {
   int64_t hot_rows;         /* BF16 mode: FP32 master rows (0: the top 1% of the vocabulary, at least 1) */
   float budget_confidence;  /* learned budget: predictions below this softmax confidence fall back (0: 0.9) */
   float budget_audit;       /* learned budget: fraction of confident vertices re-checked (0: 0.05; <0: none) */
+  int32_t autotune;         /* 1 (default): the first round picks the pair trainer's launch shape by timing */
 } felog_opts;
 
 typedef struct felog_ctx felog_ctx;
@@ -309,6 +310,9 @@ felog_status felog_write_embeddings(felog_ctx *ctx, const char *path);
 
 /* Kernels this library has launched on the context (diagnostics). */
 uint64_t felog_kernel_launches(const felog_ctx *ctx);
+/* No reference counterpart: what the launch-shape autotuner measured (per-pair time of each candidate
+ * register budget of the pair trainer) and chose, or "not tuned". */
+const char *felog_tuning_report(const felog_ctx *ctx);
 /* Device timer on the context's stream: mark(0) records the start event,
  * mark(1) the stop event; elapsed() synchronizes and returns milliseconds. */
 felog_status felog_timer_mark(felog_ctx *ctx, int which);

@@ -126,6 +126,8 @@ struct felog_ctx {
   DevBuf<int32_t> p_sen, p_negs;
   DevBuf<uint64_t> pr_count, pr_off;  // pair stream: pairs per sentence, offsets
   DevBuf<int32_t> pr_rec;             // pair stream records
+  int pair_minb = 0;                  // autotuned blocks per SM of the pair trainer (0: not tuned yet)
+  std::string tuning;                 // what the autotuner measured and chose
   DevBuf<unsigned long long> pr_cstate, pr_jump;
   DevBuf<uint32_t> pr_cfirst;
   int pr_jump_window = -1, pr_jump_k = -1;
@@ -243,6 +245,7 @@ extern "C" void felog_default_opts(felog_opts *o) {
   o->precision = FELOG_FP32;
   o->seed = 0x5EED0001ULL;
   o->slot_len = 64;
+  o->autotune = 1;
 }
 
 extern "C" felog_status felog_create(const felog_opts *opts, felog_ctx **out) {
@@ -1021,7 +1024,14 @@ void launch_trainer(felog_ctx *c, const SgArgs &g, int blocks, int threads) {
 
 template <int D, int K, class P>
 void launch_pairs_dkp(felog_ctx *c, const SgArgs &g, int blocks, int threads, uint64_t base, uint64_t s0) {
-  k_sgns_train_pairs<D, K, P><<<blocks, threads, 0, c->stream>>>(g, c->pr_rec.p, c->pr_off.p, base, s0);
+  const int minb = D >= 256 ? 2 : (c->pair_minb ? c->pair_minb : 4);
+  if (minb == 2) k_sgns_train_pairs<D, K, P, 2><<<blocks, threads, 0, c->stream>>>(g, c->pr_rec.p, c->pr_off.p, base, s0);
+  else if (minb == 3)
+    k_sgns_train_pairs<D, K, P, (D >= 256 ? 2 : 3)><<<blocks, threads, 0, c->stream>>>(g, c->pr_rec.p, c->pr_off.p, base,
+                                                                                      s0);
+  else
+    k_sgns_train_pairs<D, K, P, (D >= 256 ? 2 : 4)><<<blocks, threads, 0, c->stream>>>(g, c->pr_rec.p, c->pr_off.p, base,
+                                                                                      s0);
 }
 
 template <int K, class P>
@@ -1124,6 +1134,59 @@ felog_status train_pairs(felog_ctx *c, SgArgs g, int blocks, int threads) {
     if (K == 5) k_pair_emit<5><<<eb, 256, 0, c->stream>>>(pa);
     else k_pair_emit<7><<<eb, 256, 0, c->stream>>>(pa);
     c->launches++;
+    // launch-shape autotuner: the first chunk of the first tuned round is
+    // trained in three slices of sentences, one per candidate register budget
+    // (real work, nothing repeated); the fastest per pair is kept
+    const uint64_t nch = ch.second - ch.first;
+    if (c->o.autotune && !c->o.deterministic && c->o.size <= 128 && c->pair_minb == 0 &&
+        nch >= 3 * (uint64_t)blocks * (threads / 32)) {
+      const int cand[3] = {4, 3, 2};
+      cudaEvent_t ev[4];
+      for (int i = 0; i < 4; i++) CK(cudaEventCreate(&ev[i]), "autotune");
+      uint64_t bound[4];
+      for (int i = 0; i <= 3; i++) bound[i] = ch.first + nch * i / 3;
+      for (int i = 0; i < 3; i++) {
+        CK(cudaMemsetAsync(c->counters.p + 0, 0, 8, c->stream), "train");
+        SgArgs gi = g;
+        gi.n_sent = bound[i + 1] - bound[i];
+        c->pair_minb = cand[i];
+        CK(cudaEventRecord(ev[i], c->stream), "autotune");
+        if (K == 5) {
+          if (bf) launch_pairs_kp<5, RowsBF16>(c, gi, blocks, threads, pa.base, bound[i]);
+          else launch_pairs_kp<5, RowsF32>(c, gi, blocks, threads, pa.base, bound[i]);
+        } else {
+          if (bf) launch_pairs_kp<7, RowsBF16>(c, gi, blocks, threads, pa.base, bound[i]);
+          else launch_pairs_kp<7, RowsF32>(c, gi, blocks, threads, pa.base, bound[i]);
+        }
+        c->launches++;
+        CK(cudaGetLastError(), "train_round: launch");
+      }
+      CK(cudaEventRecord(ev[3], c->stream), "autotune");
+      uint64_t offs[4];
+      for (int i = 0; i <= 3; i++)
+        CK(cudaMemcpyAsync(&offs[i], c->pr_off.p + bound[i], 8, cudaMemcpyDeviceToHost, c->stream), "autotune");
+      CK(cudaStreamSynchronize(c->stream), "autotune");
+      double best = 1e300;
+      int pick = 4;
+      char buf[256];
+      std::string rep = "pair trainer blocks/SM:";
+      for (int i = 0; i < 3; i++) {
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, ev[i], ev[i + 1]), "autotune");
+        const double per = ms / (double)std::max<uint64_t>(1, offs[i + 1] - offs[i]);
+        snprintf(buf, sizeof buf, " %d -> %.3f ns/pair", cand[i], per * 1e6);
+        rep += buf;
+        if (per < best) {
+          best = per;
+          pick = cand[i];
+        }
+      }
+      snprintf(buf, sizeof buf, "; chose %d", pick);
+      c->tuning = rep + buf;
+      c->pair_minb = pick;
+      for (int i = 0; i < 4; i++) cudaEventDestroy(ev[i]);
+      continue;
+    }
     CK(cudaMemsetAsync(c->counters.p + 0, 0, 8, c->stream), "train");  // sentence claim counter
     g.n_sent = ch.second - ch.first;
     if (K == 5) {
@@ -1326,6 +1389,10 @@ extern "C" felog_status felog_get_embeddings(felog_ctx *c, float *syn0, float *s
 }
 
 extern "C" uint64_t felog_kernel_launches(const felog_ctx *c) { return c ? c->launches : 0; }
+
+extern "C" const char *felog_tuning_report(const felog_ctx *c) {
+  return !c ? "null context" : c->tuning.empty() ? "not tuned" : c->tuning.c_str();
+}
 
 extern "C" felog_status felog_timer_mark(felog_ctx *c, int which) {
   if (!c || (which != 0 && which != 1)) return FELOG_INVALID_ARG;

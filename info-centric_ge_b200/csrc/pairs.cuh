@@ -385,8 +385,10 @@ __device__ __forceinline__ int rec_at(const int4 (&v)[S / 4], int i) {
 // from one multi_dot and each lane evaluates one gradient; a pair whose
 // negatives repeat a row takes the sequential path, where the later target
 // sees the earlier update as in the reference.
-template <int DIM, int NK, class P>
-__global__ void __launch_bounds__(256, DIM >= 256 ? 2 : 4)
+// MINB: resident 256-thread blocks per SM the register budget is built for
+// (the launch-shape autotuner picks among 2, 3 and 4 for DIM <= 128).
+template <int DIM, int NK, class P, int MINB = (DIM >= 256 ? 2 : 4)>
+__global__ void __launch_bounds__(256, MINB)
     k_sgns_train_pairs(SgArgs a, const int32_t *__restrict__ rec, const uint64_t *__restrict__ off, uint64_t base,
                        uint64_t s0) {
   static_assert(DIM >= 64, "two or more values per lane");

@@ -44,6 +44,7 @@ class FelogOpts(ctypes.Structure):
         ("device", ctypes.c_int32), ("slot_len", ctypes.c_int32), ("seed", ctypes.c_uint64),
         ("long_arena_tokens", ctypes.c_uint64), ("wait_limit", ctypes.c_uint64),
         ("hot_rows", ctypes.c_int64), ("budget_confidence", ctypes.c_float), ("budget_audit", ctypes.c_float),
+        ("autotune", ctypes.c_int32),
     ]
 
 
@@ -160,6 +161,8 @@ def gpu_lib():
         L.felog_run.argtypes = [_P, ctypes.POINTER(RunStats)]
         L.felog_write_embeddings.argtypes = [_P, ctypes.c_char_p]
         L.felog_kernel_launches.argtypes = [_P]
+        L.felog_tuning_report.argtypes = [_P]
+        L.felog_tuning_report.restype = ctypes.c_char_p
         L.felog_kernel_launches.restype = ctypes.c_uint64
         L.felog_timer_mark.argtypes = [_P, ctypes.c_int]
         L.felog_timer_elapsed.argtypes = [_P, ctypes.POINTER(ctypes.c_float)]
@@ -444,6 +447,9 @@ class Felog:
 
     def write_embeddings(self, path):
         self._ck(self._L.felog_write_embeddings(self.h, path.encode()))
+
+    def tuning_report(self):
+        return self._L.felog_tuning_report(self.h).decode()
 
     def embeddings_into(self, syn0_ptr, n_floats):
         """Copies syn0 (vocabulary order, logical dims) into caller memory at syn0_ptr."""
