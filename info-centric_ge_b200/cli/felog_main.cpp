@@ -14,6 +14,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <unistd.h>
 #include <string>
 #include <vector>
 
@@ -22,7 +23,7 @@
 namespace {
 
 struct Cli {
-  std::string graph, partition, out_prefix, emb_output, save_vocab;
+  std::string graph, partition, out_prefix, emb_output, save_vocab, budget_model;
   bool have_v = false, have_minl = false, have_minr = false;
   bool have_alpha = false, have_cbow = false;
 };
@@ -32,10 +33,43 @@ void usage() {
           "usage: felog -g <graph.bin> -v <V> -w <walkers> --min_L <L> --min_R <R> -o <prefix>\n"
           "             [--make-undirected] [-p <partition>] [--batch_size <n>] [-r <rate>]\n"
           "             [-size n] [-window n] [-negative n] [-sample x] [-alpha x] [-cbow 0|1]\n"
-          "             [-reuse-neg 0|1] [-hs 0] [-iter n] [-min-count n] [-classes k] [-binary 0|1]\n"
+          "             [-reuse-neg 0|1|2|3] [-hs 0] [-iter n] [-min-count n] [-classes k] [-binary 0|1]\n"
           "             [-debug n] [-save-vocab f] [-emb_output f]\n"
-          "             [--use-cli-alpha] [--precision fp32|bf16] [--budget plain|learned]\n"
+          "             [--use-cli-alpha] [--precision fp32|bf16] [--budget plain|learned] [--budget-model f]\n"
           "             [--seed n] [--deterministic] [--weighted] [--max-rounds n] [--device n]\n");
+}
+
+// Budget MLP state: FELOG_MLP_STATE float32 values, as a 1-D .npy array or a
+// raw little-endian file.
+bool read_budget_model(const std::string &path, std::vector<float> &state) {
+  FILE *f = fopen(path.c_str(), "rb");
+  if (!f) return false;
+  std::vector<unsigned char> buf;
+  unsigned char tmp[65536];
+  size_t got;
+  while ((got = fread(tmp, 1, sizeof tmp, f)) > 0) buf.insert(buf.end(), tmp, tmp + got);
+  fclose(f);
+  size_t off = 0;
+  if (buf.size() >= 10 && buf[0] == 0x93 && memcmp(&buf[1], "NUMPY", 5) == 0) {
+    const int major = buf[6];
+    size_t hlen, hstart;
+    if (major == 1) {
+      hlen = buf[8] | (buf[9] << 8);
+      hstart = 10;
+    } else {
+      if (buf.size() < 12) return false;
+      hlen = buf[8] | (buf[9] << 8) | ((size_t)buf[10] << 16) | ((size_t)buf[11] << 24);
+      hstart = 12;
+    }
+    const std::string header(buf.begin() + hstart, buf.begin() + std::min(buf.size(), hstart + hlen));
+    if (header.find("<f4") == std::string::npos || header.find("'fortran_order': False") == std::string::npos)
+      return false;
+    off = hstart + hlen;
+  }
+  if (buf.size() - off != sizeof(float) * (size_t)FELOG_MLP_STATE) return false;
+  state.resize(FELOG_MLP_STATE);
+  memcpy(state.data(), buf.data() + off, sizeof(float) * (size_t)FELOG_MLP_STATE);
+  return true;
 }
 
 bool validate_partition(const std::string &path, uint32_t v_num) {
@@ -148,6 +182,7 @@ int main(int argc, char **argv) {
       else if (p == "learned") o.budget_mode = FELOG_BUDGET_LEARNED;
       else { fprintf(stderr, "felog: --budget must be plain or learned\n"); return 2; }
     }
+    else if (a == "--budget-model") cli.budget_model = need(i);
     else if (a == "--seed") o.seed = strtoull(need(i), nullptr, 10);
     else if (a == "--deterministic") o.deterministic = 1;
     else if (a == "--weighted") o.weighted = 1;
@@ -184,6 +219,24 @@ int main(int argc, char **argv) {
   if (felog_load_graph_file(ctx, cli.graph.c_str(), o.v_num, o.make_undirected) != FELOG_OK) die("load_graph");
   auto t1 = std::chrono::steady_clock::now();
   if (o.weighted && felog_build_alias(ctx) != FELOG_OK) die("build_alias");
+  if (o.budget_mode == FELOG_BUDGET_LEARNED) {
+    // default: the model shipped beside this executable
+    std::string path = cli.budget_model;
+    if (path.empty()) {
+      char exe[4096];
+      const ssize_t n = readlink("/proc/self/exe", exe, sizeof exe - 1);
+      std::string dir = n > 0 ? std::string(exe, (size_t)n) : std::string(".");
+      dir = dir.substr(0, dir.find_last_of('/') == std::string::npos ? 0 : dir.find_last_of('/'));
+      path = (dir.empty() ? std::string(".") : dir) + "/budget_mlp_c4.npy";
+    }
+    std::vector<float> state;
+    if (!read_budget_model(path, state)) {
+      fprintf(stderr, "felog: cannot read the budget model %s (%d float32 values)\n", path.c_str(), FELOG_MLP_STATE);
+      felog_destroy(ctx);
+      return 2;
+    }
+    if (felog_mlp_set_params(ctx, state.data()) != FELOG_OK) die("budget model");
+  }
   felog_run_stats rs;
   if (felog_run(ctx, &rs) != FELOG_OK) die("run");
   auto t2 = std::chrono::steady_clock::now();
