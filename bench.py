@@ -69,6 +69,8 @@ FORMS = {
     "learned-bf16-tile": dict(precision=1, budget_mode=1, reuse_neg=2),
     # FP32 tables + learned budget + center tiles
     "learned-fp32-tile": dict(precision=0, budget_mode=1, reuse_neg=2),
+    # BF16 tables + learned budget + center tiles scored on the tensor cores
+    "learned-bf16-tc": dict(precision=1, budget_mode=1, reuse_neg=3),
 }
 BUDGET_MODEL = os.path.join(ROOT, "info-centric_ge_b200", "felog_b200", "budget_mlp_c4.npy")
 METRIC = "walk+SGNS corpus tokens/s (walk steps/s and SGNS words/s reported alongside)"
@@ -349,6 +351,9 @@ def bench_mine(args):
         # center tiles: per center its contexts and the K + 1 targets, each read and written once
         sg_bytes = 2 * row_bytes * (cnt["pairs"] + (TRAIN["negative"] + 1) * cnt["kept"])
         sg_kernel = f"k_sgns_reuse_tile<128, 5, Rows{prec.upper()}>"
+    elif FORMS[form]["reuse_neg"] == 3:
+        sg_bytes = 2 * row_bytes * (cnt["pairs"] + (TRAIN["negative"] + 1) * cnt["kept"])
+        sg_kernel = "k_sgns_reuse_tile_tc<128, 5>"
     else:
         sg_bytes = cnt["pairs"] * SGNS_BYTES_PER_PAIR[prec]
         sg_kernel = f"k_sgns_train_pairs<128, 5, Rows{prec.upper()}>"
