@@ -282,7 +282,8 @@ def compare_forms(fb, g, device, model):
         wall = time.perf_counter() - t0
         out[form] = {"rounds": rs["rounds"], "walk_tokens": rs["walk_tokens"], "train_words": rs["train_words"],
                      "job_ms": rs["total_ms"], "wall_ms": wall * 1e3,
-                     "tokens_per_s": rs["walk_tokens"] / (rs["total_ms"] * 1e-3)}
+                     "tokens_per_s": rs["walk_tokens"] / (rs["total_ms"] * 1e-3),
+                     "budget": {k: rs[k] for k in ("evaluated", "predicted", "audited", "overruled")}}
         out[form]["auc"], out[form]["auc_centered"] = link_auc(f, g)
         f.close()
     p = out["plain-fp32"]

@@ -162,6 +162,10 @@ typedef struct felog_run_stats {
   double budget_ms;
   double total_ms;
   uint64_t final_unconverged;
+  uint64_t evaluated;     /* budget checks: vertices the plain criterion evaluated */
+  uint64_t predicted;     /* learned mode: vertices decided by the MLP */
+  uint64_t audited;       /* learned mode: confident predictions re-checked */
+  uint64_t overruled;     /* learned mode: audited predictions the plain criterion reversed */
 } felog_run_stats;
 
 /* ---- lifecycle ---- */

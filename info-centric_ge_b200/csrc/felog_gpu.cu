@@ -1978,6 +1978,10 @@ extern "C" felog_status felog_run(felog_ctx *c, felog_run_stats *st) {
       if (s != FELOG_OK) return s;
       rs.budget_ms += bs.ms;
       rs.final_unconverged = bs.unconverged;
+      rs.evaluated += bs.evaluated;
+      rs.predicted += bs.predicted;
+      rs.audited += bs.audited;
+      rs.overruled += bs.overruled;
       if (bs.stop_all) break;
     }
   }

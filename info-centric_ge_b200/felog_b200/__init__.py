@@ -91,7 +91,9 @@ MLP_STATE = MLP_PARAMS + 12
 class RunStats(ctypes.Structure):
     _fields_ = [("rounds", ctypes.c_uint32), ("walk_tokens", ctypes.c_uint64), ("train_words", ctypes.c_uint64),
                 ("walk_ms", ctypes.c_double), ("train_ms", ctypes.c_double), ("budget_ms", ctypes.c_double),
-                ("total_ms", ctypes.c_double), ("final_unconverged", ctypes.c_uint64)]
+                ("total_ms", ctypes.c_double), ("final_unconverged", ctypes.c_uint64),
+                ("evaluated", ctypes.c_uint64), ("predicted", ctypes.c_uint64), ("audited", ctypes.c_uint64),
+                ("overruled", ctypes.c_uint64)]
 
 
 def _struct_dict(s):
