@@ -75,6 +75,9 @@ FORMS = {
 BUDGET_MODEL = os.path.join(ROOT, "info-centric_ge_b200", "felog_b200", "budget_mlp_c4.npy")
 METRIC = "walk+SGNS corpus tokens/s (walk steps/s and SGNS words/s reported alongside)"
 WALK_BYTES_PER_STEP = 68      # 2 random 32-B sectors + 4-B token write
+# DRAM bytes per pair of k_sgns_train_pairs<128, 5> (dram__bytes_read.sum + dram__bytes_write.sum of one ncu
+# capture of the profiling case's timed round divided by its 66.0 M pairs), scaled to a launch
+DRAM_BYTES_PER_PAIR = {"fp32": 1059.2, "bf16": 234.2}
 SGNS_BYTES_PER_PAIR = {"fp32": 7168,   # 14 rows x 128 x 4 B (read + write syn0 row and 6 syn1 rows)
                        "bf16": 3584}   # the same rows at 2 B per value (FP32 master rows: top 1%)
 
@@ -238,9 +241,9 @@ def cpu_baseline(g, cfg):
             "walk_steps_per_s": walk_rate, "sgns_words_per_s": train_rate}
 
 
-def new_context(fb, g, form, device, seed, model):
+def new_context(fb, g, form, device, seed, model, autotune=1):
     V = g["v_num"]
-    f = fb.Felog(v_num=V, device=device, seed=seed, **{**TRAIN, **FORMS[form]})
+    f = fb.Felog(v_num=V, device=device, seed=seed, autotune=autotune, **{**TRAIN, **FORMS[form]})
     f.load_graph(g["edges"], V)
     f.init_model()
     if FORMS[form]["budget_mode"] == 1:
@@ -303,7 +306,7 @@ def bench_mine(args):
     form = args.form
     prec = "bf16" if FORMS[form]["precision"] else "fp32"
     model = np.load(args.budget_model) if FORMS[form]["budget_mode"] or not args.no_forms else None
-    f = new_context(fb, g, form, local, 1000 + rank, model)
+    f = new_context(fb, g, form, local, 1000 + rank, model, autotune=0 if args.no_autotune else 1)
     min_r = TRAIN["min_rounds"]
     warm = {k: 0.0 for k in ("tokens", "words", "pairs", "kept", "walk_ms", "train_ms", "plan_ms", "budget_ms")}
     for r in range(args.warmup):
@@ -385,8 +388,11 @@ def bench_mine(args):
         "phase_ms_per_step": {k: cnt[k] / args.steps for k in ("walk_ms", "plan_ms", "train_ms", "budget_ms")},
         "tokens_per_step": cnt["tokens"] / args.steps,
         "pairs_per_step": cnt["pairs"] / args.steps,
-        "roofline": {"kernel": sg_kernel, "bound": "hbm", "achieved": sg_achieved, "peak": peak,
-                     "unit": "GB/s", "frac": sg_achieved / peak, "traffic": None,
+        "roofline": {"kernel": sg_kernel, "bound": "hbm",
+                     "traffic": (DRAM_BYTES_PER_PAIR[prec] * cnt["pairs"] / args.steps
+                                 if FORMS[form]["reuse_neg"] == 0 else None),
+                     "traffic_unit": "bytes per launch (ncu per-pair DRAM traffic x pairs per launch)", "achieved": sg_achieved, "peak": peak,
+                     "unit": "GB/s", "frac": sg_achieved / peak,
                      "peak_source": peak_kind,
                      "walk_kernel": {"achieved": walk_achieved, "frac": walk_achieved / peak,
                                      "bytes_per_step": WALK_BYTES_PER_STEP}},
@@ -471,6 +477,8 @@ def main():
     ap.add_argument("--form", default="learned-bf16", choices=sorted(FORMS))
     ap.add_argument("--budget-model", default=BUDGET_MODEL)
     ap.add_argument("--no-forms", action="store_true", help="skip the end-to-end plain vs learned comparison")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the default launch shape (profiling: a tuner timed under ncu is distorted)")
     args = ap.parse_args()
     if args.impl == "reference":
         bench_reference(args)
