@@ -234,6 +234,15 @@ felog_status felog_train_round(felog_ctx *ctx, uint32_t round, float alpha, felo
 /* rows in vocabulary order, logical dimension order, FP32 */
 felog_status felog_get_embeddings(felog_ctx *ctx, float *syn0, float *syn1, uint64_t cap_floats);
 felog_status felog_set_embeddings(felog_ctx *ctx, const float *syn0, const float *syn1);
+/* syn0 as felog_get_embeddings returns it, copied to host memory behind the
+ * caller's back: the call enqueues a device snapshot and a device-to-host copy
+ * on a second stream and returns, so the copy overlaps the next round (the
+ * reference copies syn0 back after every round, word2vec.cu:1264, while its
+ * trainer waits).  The buffer must stay valid, and should be pinned for the
+ * copy to be asynchronous, until felog_wait_embeddings returns.  A later call
+ * is ordered after the previous copy. */
+felog_status felog_copy_embeddings_async(felog_ctx *ctx, float *syn0, uint64_t cap_floats);
+felog_status felog_wait_embeddings(felog_ctx *ctx);
 /* No counterpart in the reference (precision study).  For n (context row,
  * target row, label) triples in vocabulary-row indices: dots[i] = the FP32
  * dot of syn0[ctx] and syn1[target] formed exactly as the trainer forms it

@@ -66,6 +66,10 @@ struct felog_ctx {
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   cudaEvent_t tm0 = nullptr, tm1 = nullptr;  // user timer (felog_timer_mark)
+  // asynchronous embedding copies (felog_copy_embeddings_async)
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t copy_ready = nullptr, copy_done = nullptr;
+  bool copy_pending = false;
   std::string err;
   int sm_count = 148;
 
@@ -151,6 +155,12 @@ struct felog_ctx {
   // cub scratch, output staging, launch count of this library's kernels
   DevBuf<unsigned char> cub_tmp;
   DevBuf<float> out_tmp;
+  DevBuf<float> copy_stage;  // syn0 snapshot being copied to the host
+  // pinned, device-mapped host buffer for the small readbacks of a round (counts,
+  // offsets, flags): a kernel writes it, so a readback never waits behind a bulk
+  // copy that occupies the device-to-host copy engine
+  uint8_t *mbox = nullptr;
+  size_t mbox_cap = 0;
   uint64_t launches = 0;
 };
 
@@ -188,10 +198,61 @@ int grid_for(felog_ctx *c, uint64_t n, int threads, int per_sm = 8) {
   return (int)g;
 }
 
+// Copies device bytes into the mapped host buffer with plain stores: 16- or
+// 4-byte words as far as the source alignment allows, the rest byte by byte.
+__global__ void k_to_host(const void *src, void *dst, uint64_t bytes) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  const uint64_t t0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint64_t a = (uint64_t)(uintptr_t)src;
+  uint64_t body = 0;
+  if ((a & 15) == 0) {
+    body = bytes & ~(uint64_t)15;
+    const uint4 *s = static_cast<const uint4 *>(src);
+    uint4 *d = static_cast<uint4 *>(dst);
+    for (uint64_t i = t0; i < body / 16; i += stride) d[i] = s[i];
+  } else if ((a & 3) == 0) {
+    body = bytes & ~(uint64_t)3;
+    const uint32_t *s = static_cast<const uint32_t *>(src);
+    uint32_t *d = static_cast<uint32_t *>(dst);
+    for (uint64_t i = t0; i < body / 4; i += stride) d[i] = s[i];
+  }
+  const uint8_t *s = static_cast<const uint8_t *>(src);
+  uint8_t *d = static_cast<uint8_t *>(dst);
+  for (uint64_t i = body + t0; i < bytes; i += stride) d[i] = s[i];
+}
+
+// Synchronous readback of `bytes` device bytes on the context's stream, through
+// the mapped host buffer (grown on demand, in 64 KiB steps).
+felog_status readback(felog_ctx *c, void *dst, const void *dsrc, size_t bytes, const char *what) {
+  if (!bytes) return FELOG_OK;
+  if (bytes > c->mbox_cap) {
+    CK(cudaStreamSynchronize(c->stream), what);
+    if (c->mbox) CK(cudaFreeHost(c->mbox), what);
+    c->mbox = nullptr;
+    c->mbox_cap = 0;
+    const size_t cap = (bytes + 65535) & ~(size_t)65535;
+    CK(cudaHostAlloc((void **)&c->mbox, cap, cudaHostAllocMapped), what);
+    c->mbox_cap = cap;
+  }
+  void *dmb = nullptr;
+  CK(cudaHostGetDevicePointer(&dmb, c->mbox, 0), what);
+  k_to_host<<<grid_for(c, (bytes + 15) / 16, 256), 256, 0, c->stream>>>(dsrc, dmb, bytes);
+  c->launches++;
+  CK(cudaGetLastError(), what);
+  CK(cudaStreamSynchronize(c->stream), what);
+  memcpy(dst, c->mbox, bytes);
+  return FELOG_OK;
+}
+
+#define RB(dst, src, bytes, what)                              \
+  do {                                                         \
+    felog_status _s = readback(c, (dst), (src), (bytes), what); \
+    if (_s != FELOG_OK) return _s;                             \
+  } while (0)
+
 felog_status check_dev_err(felog_ctx *c, const char *what) {
   int h = 0;
-  CK(cudaMemcpyAsync(&h, c->derr.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream), what);
-  CK(cudaStreamSynchronize(c->stream), what);
+  RB(&h, c->derr.p, sizeof(int), what);
   if (h == kErrNone) return FELOG_OK;
   CK(cudaMemsetAsync(c->derr.p, 0, sizeof(int), c->stream), what);
   switch (h) {
@@ -285,7 +346,13 @@ extern "C" felog_status felog_create(const felog_opts *opts, felog_ctx **out) {
 extern "C" void felog_destroy(felog_ctx *c) {
   if (!c) return;
   cudaSetDevice(c->device);
+  if (c->copy_pending && c->copy_done) cudaEventSynchronize(c->copy_done);
+  if (c->copy_ready) cudaEventDestroy(c->copy_ready);
+  if (c->copy_done) cudaEventDestroy(c->copy_done);
+  if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
+  c->copy_stage.release();
   if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->mbox) cudaFreeHost(c->mbox);
   c->row_ptr.release(); c->adj.release(); c->deg.release(); c->alias_prob.release(); c->alias_idx.release();
   c->stop.release(); c->active.release(); c->arena.release(); c->sent_ptr.release(); c->sent_len.release();
   c->visit_freq.release(); c->counters.release(); c->derr.release(); c->inj_idx_off.release();
@@ -471,7 +538,8 @@ extern "C" felog_status felog_set_stop_flags(felog_ctx *c, const uint8_t *flags)
 extern "C" felog_status felog_get_stop_flags(felog_ctx *c, uint8_t *flags) {
   if (!c || !flags) return FELOG_INVALID_ARG;
   if (!c->V) return fail(c, FELOG_NOT_READY, "no graph loaded");
-  CK(cudaMemcpy(flags, c->stop.p, c->V, cudaMemcpyDeviceToHost), "get_stop_flags");
+  CK(cudaSetDevice(c->device), "get_stop_flags");
+  RB(flags, c->stop.p, c->V, "get_stop_flags");
   return FELOG_OK;
 }
 
@@ -503,8 +571,7 @@ felog_status build_active(felog_ctx *c, uint32_t walker_num) {
   k_active_scatter<<<grid_for(c, walker_num, 256), 256, 0, c->stream>>>(flag, pos, walker_num, c->active.p);
   c->launches++;
   uint32_t na = 0;
-  CK(cudaMemcpyAsync(&na, pos + walker_num, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream), "walk_round");
-  CK(cudaStreamSynchronize(c->stream), "walk_round");
+  RB(&na, pos + walker_num, sizeof(uint32_t), "walk_round");
   c->n_active = na;
   return FELOG_OK;
 }
@@ -547,8 +614,7 @@ felog_status round_kl(felog_ctx *c, double *out) {
   c->launches++;
   k_kl_final<<<1, 32, 0, c->stream>>>(c->kl_partial.p, nb, c->kl_partial.p + nb);
   c->launches++;
-  CK(cudaMemcpyAsync(out, c->kl_partial.p + nb, sizeof(double), cudaMemcpyDeviceToHost, c->stream), "kl");
-  CK(cudaStreamSynchronize(c->stream), "kl");
+  RB(out, c->kl_partial.p + nb, sizeof(double), "kl");
   return FELOG_OK;
 }
 
@@ -643,7 +709,7 @@ extern "C" felog_status felog_walk_round(felog_ctx *c, uint32_t round, const fel
   }
   CK(cudaEventRecord(c->ev1, c->stream), "walk_round");
   unsigned long long h[16];
-  CK(cudaMemcpyAsync(h, c->counters.p, sizeof h, cudaMemcpyDeviceToHost, c->stream), "walk_round");
+  RB(h, c->counters.p, sizeof h, "walk_round");
   s = check_dev_err(c, "walk_round");
   if (s != FELOG_OK) return s;
   float ms = 0;
@@ -983,10 +1049,9 @@ felog_status plan_round(felog_ctx *c, float *ms) {
   CK(cub::DeviceScan::ExclusiveSum(c->cub_tmp.p, tmp, c->p_kept.p, c->p_out_off.p, (int)(n + 1), c->stream),
      "plan");
   uint64_t total = 0, nb = 0;
-  CK(cudaMemcpyAsync(&total, c->p_out_off.p + n, 8, cudaMemcpyDeviceToHost, c->stream), "plan");
+  RB(&total, c->p_out_off.p + n, 8, "plan");
   unsigned long long hc[2];
-  CK(cudaMemcpyAsync(hc, c->counters.p + 4, sizeof hc, cudaMemcpyDeviceToHost, c->stream), "plan");
-  CK(cudaStreamSynchronize(c->stream), "plan");
+  RB(hc, c->counters.p + 4, sizeof hc, "plan");
   nb = hc[0];
   CK(c->p_sen.ensure(total + 1), "plan");
   a.sen = c->p_sen.p;
@@ -1102,15 +1167,14 @@ felog_status train_pairs(felog_ctx *c, SgArgs g, int blocks, int threads) {
   CK(cub::DeviceScan::ExclusiveSum(c->cub_tmp.p, tmp, c->pr_count.p, c->pr_off.p, (int)(n + 1), c->stream),
      "train");
   uint64_t total = 0;
-  CK(cudaMemcpyAsync(&total, c->pr_off.p + n, 8, cudaMemcpyDeviceToHost, c->stream), "train");
-  CK(cudaStreamSynchronize(c->stream), "train");
+  RB(&total, c->pr_off.p + n, 8, "train");
   // chunks of whole sentences
   std::vector<std::pair<uint64_t, uint64_t>> chunks;
   if (total <= kPairChunk) {
     chunks.push_back({0, n});
   } else {
     c->h_pr_off.resize(n + 1);
-    CK(cudaMemcpy(c->h_pr_off.data(), c->pr_off.p, 8 * (n + 1), cudaMemcpyDeviceToHost), "train");
+    RB(c->h_pr_off.data(), c->pr_off.p, 8 * (n + 1), "train");
     uint64_t s0 = 0;
     while (s0 < n) {
       uint64_t s1 = s0 + 1;
@@ -1163,9 +1227,7 @@ felog_status train_pairs(felog_ctx *c, SgArgs g, int blocks, int threads) {
       }
       CK(cudaEventRecord(ev[3], c->stream), "autotune");
       uint64_t offs[4];
-      for (int i = 0; i <= 3; i++)
-        CK(cudaMemcpyAsync(&offs[i], c->pr_off.p + bound[i], 8, cudaMemcpyDeviceToHost, c->stream), "autotune");
-      CK(cudaStreamSynchronize(c->stream), "autotune");
+      for (int i = 0; i <= 3; i++) RB(&offs[i], c->pr_off.p + bound[i], 8, "autotune");
       double best = 1e300;
       int pick = 4;
       char buf[256];
@@ -1302,7 +1364,7 @@ extern "C" felog_status felog_train_round(felog_ctx *c, uint32_t round, float al
   }
   CK(cudaEventRecord(c->ev1, c->stream), "train_round");
   unsigned long long h[4];
-  CK(cudaMemcpyAsync(h, c->counters.p, sizeof h, cudaMemcpyDeviceToHost, c->stream), "train_round");
+  RB(h, c->counters.p, sizeof h, "train_round");
   s = check_dev_err(c, "train_round");
   if (s != FELOG_OK) return s;
   CK(cudaEventElapsedTime(&ms_train, c->ev0, c->ev1), "train_round");
@@ -1311,7 +1373,7 @@ extern "C" felog_status felog_train_round(felog_ctx *c, uint32_t round, float al
     // words considered = sum of considered tokens per sentence
     std::vector<uint32_t> cons(c->plan_sent);
     if (c->plan_sent)
-      CK(cudaMemcpy(cons.data(), c->p_cons.p, 4 * c->plan_sent, cudaMemcpyDeviceToHost), "train_round");
+      RB(cons.data(), c->p_cons.p, 4 * (size_t)c->plan_sent, "train_round");
     uint64_t w = 0;
     for (uint32_t x : cons) w += x;
     stats->words = w;
@@ -1385,6 +1447,45 @@ extern "C" felog_status felog_get_embeddings(felog_ctx *c, float *syn0, float *s
     CK(cudaMemcpyAsync(dst, c->out_tmp.p, 4 * nel, cudaMemcpyDeviceToHost, c->stream), "get_embeddings");
     CK(cudaStreamSynchronize(c->stream), "get_embeddings");
   }
+  return FELOG_OK;
+}
+
+extern "C" felog_status felog_copy_embeddings_async(felog_ctx *c, float *syn0, uint64_t cap_floats) {
+  if (!c || !syn0) return FELOG_INVALID_ARG;
+  if (!c->model_ready) return fail(c, FELOG_NOT_READY, "model not initialised");
+  const int dim = c->o.size;
+  const uint64_t nel = (uint64_t)c->vocab_size * dim;
+  if (cap_floats < nel)
+    return fail(c, FELOG_INVALID_ARG, "copy_embeddings_async: need %llu floats", (unsigned long long)nel);
+  CK(cudaSetDevice(c->device), "copy_embeddings_async");
+  if (!c->copy_stream) {
+    CK(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking), "copy_embeddings_async");
+    CK(cudaEventCreateWithFlags(&c->copy_ready, cudaEventDisableTiming), "copy_embeddings_async");
+    CK(cudaEventCreateWithFlags(&c->copy_done, cudaEventDisableTiming), "copy_embeddings_async");
+  }
+  CK(c->copy_stage.ensure(nel), "copy_embeddings_async");
+  // the staging buffer is rewritten only after the previous copy has left it
+  if (c->copy_pending) CK(cudaStreamWaitEvent(c->stream, c->copy_done, 0), "copy_embeddings_async");
+  k_unpermute<<<grid_for(c, nel, 256), 256, 0, c->stream>>>(c->syn0.p, c->syn0_bf.p, (uint64_t)c->n_f32,
+                                                             c->copy_stage.p, (uint64_t)c->vocab_size, dim);
+  c->launches++;
+  CK(cudaGetLastError(), "copy_embeddings_async");
+  CK(cudaEventRecord(c->copy_ready, c->stream), "copy_embeddings_async");
+  CK(cudaStreamWaitEvent(c->copy_stream, c->copy_ready, 0), "copy_embeddings_async");
+  CK(cudaMemcpyAsync(syn0, c->copy_stage.p, 4 * nel, cudaMemcpyDeviceToHost, c->copy_stream),
+     "copy_embeddings_async");
+  CK(cudaEventRecord(c->copy_done, c->copy_stream), "copy_embeddings_async");
+  c->copy_pending = true;
+  return FELOG_OK;
+}
+
+extern "C" felog_status felog_wait_embeddings(felog_ctx *c) {
+  if (!c) return FELOG_INVALID_ARG;
+  if (!c->copy_pending) return FELOG_OK;
+  CK(cudaEventSynchronize(c->copy_done), "wait_embeddings");
+  // later work on the context's stream (and its timer events) comes after the copy
+  CK(cudaStreamWaitEvent(c->stream, c->copy_done, 0), "wait_embeddings");
+  c->copy_pending = false;
   return FELOG_OK;
 }
 
@@ -1554,8 +1655,7 @@ extern "C" felog_status felog_budget_check(felog_ctx *c, uint32_t round, felog_b
   CK(cudaGetLastError(), "budget_check");
   CK(cudaEventRecord(c->ev1, c->stream), "budget_check");
   unsigned long long h[8];
-  CK(cudaMemcpyAsync(h, c->counters.p, sizeof h, cudaMemcpyDeviceToHost, c->stream), "budget_check");
-  CK(cudaStreamSynchronize(c->stream), "budget_check");
+  RB(h, c->counters.p, sizeof h, "budget_check");
   float ms = 0;
   CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1), "budget_check");
   // eva_num ratio test (word2vec.cu:2073-2080); the first comparison is against

@@ -163,6 +163,8 @@ def gpu_lib():
         L.felog_run.argtypes = [_P, ctypes.POINTER(RunStats)]
         L.felog_write_embeddings.argtypes = [_P, ctypes.c_char_p]
         L.felog_kernel_launches.argtypes = [_P]
+        L.felog_copy_embeddings_async.argtypes = [_P, _P, ctypes.c_uint64]
+        L.felog_wait_embeddings.argtypes = [_P]
         L.felog_tuning_report.argtypes = [_P]
         L.felog_tuning_report.restype = ctypes.c_char_p
         L.felog_kernel_launches.restype = ctypes.c_uint64
@@ -449,6 +451,13 @@ class Felog:
 
     def write_embeddings(self, path):
         self._ck(self._L.felog_write_embeddings(self.h, path.encode()))
+
+    def embeddings_into_async(self, syn0_ptr, n_floats):
+        """Starts copying syn0 into caller memory (pinned) behind the next round; finish with wait_embeddings()."""
+        self._ck(self._L.felog_copy_embeddings_async(self.h, syn0_ptr, n_floats))
+
+    def wait_embeddings(self):
+        self._ck(self._L.felog_wait_embeddings(self.h))
 
     def tuning_report(self):
         return self._L.felog_tuning_report(self.h).decode()

@@ -67,3 +67,33 @@ def test_stopped_vertices_spawn_no_walkers():
     tok, off = f.corpus()
     assert st["n_sentences"] == V - V // 2
     assert (tok[off[:-1].astype(np.int64)] >= V // 2).all()
+
+
+def test_async_embedding_copy_equals_sync_copy():
+    """felog_copy_embeddings_async snapshots syn0 at the call: after another
+    round has run, the host buffer holds the rows of the earlier round, equal
+    to a synchronous felog_get_embeddings taken at the same point."""
+    import ctypes
+
+    import torch
+
+    g = fb.synth_graph(seed=4, v_target=4096, e_target=32768, holdout=0.0)
+    V = g["v_num"]
+    f = fb.Felog(v_num=V, size=128, window=5, negative=5, sample=1e-3, cbow=0, reuse_neg=0, min_count=0, seed=3)
+    f.load_graph(g["edges"], V)
+    f.init_model()
+    f.walk_round(0)
+    f.train_round(0)
+    sync0, _ = f.embeddings()
+    vs = f.vocab()[2]
+    buf = torch.zeros(vs * 128, dtype=torch.float32).pin_memory()
+    f.embeddings_into_async(ctypes.c_void_p(buf.data_ptr()), vs * 128)
+    f.walk_round(1)
+    f.train_round(1)  # runs while (or after) the copy of round 0's rows
+    f.wait_embeddings()
+    np.testing.assert_array_equal(buf.numpy(), sync0)
+    sync1, _ = f.embeddings()
+    assert not np.array_equal(sync1, sync0)
+    f.embeddings_into_async(ctypes.c_void_p(buf.data_ptr()), vs * 128)
+    f.wait_embeddings()
+    np.testing.assert_array_equal(buf.numpy(), sync1)

@@ -32,9 +32,9 @@ def graph4096():
     return fx["edges"], int(fx["V"])
 
 
-def trainer(dim=128, window=10, negative=5, sample=1e-3, reuse_neg=0, **kw):
+def trainer(dim=128, window=10, negative=5, sample=1e-3, reuse_neg=0, cbow=0, **kw):
     e, V = graph4096()
-    f = fb.Felog(v_num=V, size=dim, window=window, negative=negative, sample=sample, cbow=0, reuse_neg=reuse_neg,
+    f = fb.Felog(v_num=V, size=dim, window=window, negative=negative, sample=sample, cbow=cbow, reuse_neg=reuse_neg,
                  min_count=0, **kw)
     f.load_graph(e, V)
     f.init_model()
@@ -231,3 +231,21 @@ def test_reuse_neg_deterministic_matches_oracle(dim, negative):
                           pl["negs"], 5, dim, negative, 0.025)
     exact = np.mean(g0 == syn0), np.mean(g1 == syn1)
     assert exact == (1.0, 1.0), f"fraction bit-exact syn0/syn1: {exact}"
+
+
+@pytest.mark.parametrize("dim,negative", [(128, 5), (64, 3)])
+def test_cbow_deterministic_matches_oracle(dim, negative):
+    """-cbow 1 (cbow_kernel, word2vec.cu:538-646) in the one-warp mode, FP32
+    form, against the oracle's sequential restatement."""
+    f, e, V = trainer(dim=dim, window=5, negative=negative, sample=1e-3, deterministic=1, cbow=1)
+    tok, off = walk_corpus(V, e, seed=13)
+    n = 300
+    tok, off = tok[: int(off[n])], off[: n + 1]
+    f.set_corpus(tok, off)
+    f.train_round(0, alpha=0.05)
+    g0, g1 = f.embeddings()
+    r0, r1 = oracle_train(f, e, V, tok, off, dim, 5, negative, 1e-3, 0.05, cbow=True)
+    np.testing.assert_allclose(g0, r0, rtol=RTOL, atol=1e-7)
+    np.testing.assert_allclose(g1, r1, rtol=RTOL, atol=1e-7)
+    exact = np.mean(g0 == r0), np.mean(g1 == r1)
+    print("cbow fraction bit-exact syn0/syn1:", exact)
