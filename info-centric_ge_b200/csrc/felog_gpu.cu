@@ -98,7 +98,7 @@ struct felog_ctx {
   DevBuf<unsigned int> visit_freq;
   uint64_t words_sum_cum = 0;
   DevBuf<unsigned long long> counters;  // scratch counters
-  DevBuf<unsigned int> walk_claim;     // walker claim counters
+  DevBuf<unsigned int> walk_claim;     // walker claim counter
   DevBuf<int> derr;
   DevBuf<uint64_t> inj_idx_off, inj_p_off;
   DevBuf<uint32_t> inj_idx;
@@ -106,6 +106,7 @@ struct felog_ctx {
   DevBuf<uint32_t> flags_tmp;
   DevBuf<double> kl_partial;
   DevBuf<double> corr_tab;
+  DevBuf<double4> corr_series;
   bool corr_tab_ready = false;
 
   // vocabulary / model
@@ -357,7 +358,7 @@ extern "C" void felog_destroy(felog_ctx *c) {
   c->stop.release(); c->active.release(); c->arena.release(); c->sent_ptr.release(); c->sent_len.release();
   c->visit_freq.release(); c->counters.release(); c->derr.release(); c->inj_idx_off.release();
   c->inj_p_off.release(); c->inj_idx.release(); c->inj_p.release(); c->flags_tmp.release();
-  c->kl_partial.release(); c->corr_tab.release(); c->id2offset.release(); c->thr.release(); c->table.release();
+  c->kl_partial.release(); c->corr_tab.release(); c->corr_series.release(); c->id2offset.release(); c->thr.release(); c->table.release();
   c->exp_table.release(); c->syn0.release(); c->syn1.release(); c->syn0_bf.release(); c->syn1_bf.release(); c->jump.release();
   c->p_cand.release(); c->p_draws.release(); c->p_cons.release(); c->p_kept.release(); c->p_blk.release();
   c->p_state.release(); c->p_neg_state.release(); c->p_out_off.release(); c->p_batch_first.release();
@@ -662,6 +663,9 @@ extern "C" felog_status felog_walk_round(felog_ctx *c, uint32_t round, const fel
     CK(c->corr_tab.ensure((kCorrTableS + 1) * (kCorrTableS + 1)), "walk_round: correlation table");
     k_corr_table<<<64, 256, 0, c->stream>>>(c->corr_tab.p);
     c->launches++;
+    CK(c->corr_series.ensure(kCorrSeries), "walk_round: correlation series");
+    k_corr_series<<<1, 32, 0, c->stream>>>(c->corr_series.p);
+    c->launches++;
     CK(cudaGetLastError(), "walk_round: correlation table");
     c->corr_tab_ready = true;
   }
@@ -693,17 +697,21 @@ extern "C" felog_status felog_walk_round(felog_ctx *c, uint32_t round, const fel
   a.sent_len = c->sent_len.p;
   a.visit_freq = c->visit_freq.p;
   a.corr_tab = c->corr_tab.p;
-  CK(c->walk_claim.ensure(kWalkClaimers), "walk_round");
-  CK(cudaMemsetAsync(c->walk_claim.p, 0, 4 * kWalkClaimers, c->stream), "walk_round");
+  a.corr_series = c->corr_series.p;
+  CK(c->walk_claim.ensure(1), "walk_round");
+  CK(cudaMemsetAsync(c->walk_claim.p, 0, 4, c->stream), "walk_round");
   a.next_walker = c->walk_claim.p;
   a.stats = c->counters.p;
   a.err = c->derr.p;
   CK(cudaEventRecord(c->ev0, c->stream), "walk_round");
   if (na) {
-    int blocks = c->sm_count * 8;
-    if (a.injected) k_walk<true, false><<<blocks, 256, 0, c->stream>>>(a);
-    else if (a.weighted) k_walk<false, true><<<blocks, 256, 0, c->stream>>>(a);
-    else k_walk<false, false><<<blocks, 256, 0, c->stream>>>(a);
+    // persistent grid: exactly the blocks that are resident at once, so no
+    // block waits for a slot only to find every walker claimed
+    void (*kern)(WalkArgs) = a.injected ? k_walk<true, false> : a.weighted ? k_walk<false, true> : k_walk<false, false>;
+    int per_sm = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kWalkThreads, 0), "walk_round: occupancy");
+    const int blocks = c->sm_count * std::max(per_sm, 1);
+    kern<<<blocks, kWalkThreads, 0, c->stream>>>(a);
     c->launches++;
     CK(cudaGetLastError(), "walk_round: launch");
   }

@@ -1,5 +1,8 @@
-// Walker engine: one lane per walker, persistent grid, walkers claimed from a
-// global counter so uneven walks keep every lane busy.
+// Walker engine: one lane per walker, persistent grid sized to residency;
+// each warp claims 32 consecutive walkers with one atomic, so uneven walks keep
+// every warp busy.  The round's counters are summed per warp before the
+// single atomic per counter: same-address atomics from every thread at exit
+// serialize in L2 and once cost more than the walks themselves.
 //
 // Per walker it restates walk.hpp:926-1101 at np = 1:
 //   * step 0 is the start vertex; the first visit seeds the correlation state
@@ -14,12 +17,23 @@
 //     R^2 < 0.999 or R < 0 (:945-951, :1056-1062, :1088-1093).
 // The +,-,*,/ of the correlation update are IEEE intrinsics so the compiler
 // cannot contract them; pow/log2/tanh/sqrt are the FP64 device functions.
+// Three exact shortcuts keep the per-token FP64 work small:
+//   * E[S], E[S^2] and D_S depend only on S, so they come from a table built
+//     once with the same operations (k_corr_series);
+//   * a division by the integer S + 1 is Markstein's correction of the
+//     product with the correctly rounded reciprocal (the table holds it),
+//     which is the correctly rounded quotient; tiny dividends take __ddiv_rn;
+//   * R is formed only when the stop test can fire (step > min_L).
+// The trace test tanh(p_accept) <= p first runs in FP32: tanhf of the FP32
+// p_accept is within 3e-7 of the FP64 tanh while degrees stay below 2^24, so
+// a gap of more than 2^-16 to p decides it; otherwise the FP64 test runs.
 //
 // Tokens go to a per-walker slot of slot_len tokens; a walk that outgrows it
-// moves to a doubled chunk of the spill arena.  fi lookups use a 64-bit
-// Bloom word per walker (no scan for first visits) and a scan of the walk's
-// own tokens otherwise; the return step of a trace uses a running count of
-// the current vertex.
+// moves to a doubled chunk of the spill arena.  The first kSmemPath tokens of
+// each walk are also kept in shared memory.  fi lookups use a 64-bit Bloom
+// word per walker (no scan for first visits) and a scan of the walk's own
+// tokens otherwise (shared memory first, the global tail after it); the
+// return step of a trace uses a running count of the current vertex.
 #pragma once
 
 #include "common.cuh"
@@ -54,19 +68,19 @@ struct WalkArgs {
   uint32_t *sent_len;
   unsigned int *visit_freq;      // cumulative visits per vertex (KL)
   const double *corr_tab;        // t(S, fi) table (k_corr_table), or NULL
-  unsigned int *next_walker;     // kWalkClaimers claim counters (walker i + kWalkClaimers j)
+  const double4 *corr_series;    // S-only moments and reciprocals (k_corr_series)
+  unsigned int *next_walker;     // claim counter: next unclaimed walker index
   unsigned long long *stats;     // [tokens, traces, iterations, long]
   int *err;
 };
 
-constexpr uint32_t kWalkClaimers = 64;  // claim counters: walkers i, i + 64, i + 128, ... share counter i
-
 struct Corr {
-  double H, EH, ES, EHS, EHH, ESS, R, S;  // N == S throughout (both count tokens)
+  double H, EH, ES, EHS, EHH, ESS, S;  // N == S throughout (both count tokens)
 };
 
+// ES and ESS are only kept current once S leaves the series table.
 __device__ __forceinline__ void corr_init(Corr &c) {
-  c.H = 0.0; c.EH = 0.0; c.ES = 1.0; c.EHS = 0.0; c.EHH = 0.0; c.ESS = 1.0; c.R = 1.0; c.S = 1.0;
+  c.H = 0.0; c.EH = 0.0; c.ES = 1.0; c.EHS = 0.0; c.EHH = 0.0; c.ESS = 1.0; c.S = 1.0;
 }
 
 // The entropy increment t(S, fi) of Correlation::iterateHn with step_k = 1
@@ -95,29 +109,85 @@ __global__ void k_corr_table(double *tab) {
   }
 }
 
-// Correlation::iterate with step_k = 1 (walk.hpp:309-366).
-__device__ __forceinline__ void corr_iterate(Corr &c, uint32_t fi_u, const double *__restrict__ tab) {
-  const double Sn = c.S;
-  const double Snp1 = __dadd_rn(Sn, 1.0);
-  const double fi = (double)fi_u;
-  const uint32_t S_u = (uint32_t)Sn;
-  const double t = (tab && S_u <= (uint32_t)kCorrTableS) ? __ldg(&tab[corr_tab_index(S_u, fi_u)]) : corr_t(Sn, fi);
-  const double H1 = __ddiv_rn(__dsub_rn(__dmul_rn(Sn, c.H), t), Snp1);
-  const double Np1 = Snp1;  // N + 1 with N == S
-  const double EH = __dadd_rn(c.EH, __ddiv_rn(__dsub_rn(H1, c.EH), Np1));
-  const double ES = __dadd_rn(c.ES, __ddiv_rn(__dsub_rn(Snp1, c.ES), Np1));
-  const double EHS = __dadd_rn(c.EHS, __ddiv_rn(__dsub_rn(__dmul_rn(H1, Snp1), c.EHS), Np1));
-  const double EHH = __dadd_rn(c.EHH, __ddiv_rn(__dsub_rn(__dmul_rn(H1, H1), c.EHH), Np1));
-  const double ESS = __dadd_rn(c.ESS, __ddiv_rn(__dsub_rn(__dmul_rn(Snp1, Snp1), c.ESS), Np1));
-  const double DH = __dsub_rn(EHH, __dmul_rn(EH, EH));
-  const double DS = __dsub_rn(ESS, __dmul_rn(ES, ES));
-  const double ex = __dsub_rn(EHS, __dmul_rn(EH, ES));
-  c.R = ex == 0.0 ? 0.0 : __ddiv_rn(ex, __dsqrt_rn(__dmul_rn(DH, DS)));
-  c.H = H1; c.EH = EH; c.ES = ES; c.EHS = EHS; c.EHH = EHH; c.ESS = ESS; c.S = Snp1;
+// Series of the S-only moments: entry s = {E[S], E[S^2], D_S, RN(1/(s+1))}
+// after the update that takes S from s to s + 1 (walk.hpp:322-366 with
+// step_k = 1), for 1 <= s < kCorrSeries; one thread, the walker's operations.
+constexpr uint32_t kCorrSeries = 256;
+
+__global__ void k_corr_series(double4 *ser) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  double ES = 1.0, ESS = 1.0;
+  ser[0] = make_double4(ES, ESS, 0.0, 1.0);
+  for (uint32_t s = 1; s < kCorrSeries; s++) {
+    const double Snp1 = __dadd_rn((double)s, 1.0);
+    ES = __dadd_rn(ES, __ddiv_rn(__dsub_rn(Snp1, ES), Snp1));
+    ESS = __dadd_rn(ESS, __ddiv_rn(__dsub_rn(__dmul_rn(Snp1, Snp1), ESS), Snp1));
+    ser[s] = make_double4(ES, ESS, __dsub_rn(ESS, __dmul_rn(ES, ES)), __drcp_rn(Snp1));
+  }
 }
 
-__device__ __forceinline__ bool corr_stop(const Corr &c, uint32_t step, uint32_t min_len) {
-  return step > min_len && (__dmul_rn(c.R, c.R) < 0.999 || c.R < 0.0);
+// x / n rounded to nearest for n an integer-valued double and y = RN(1/n):
+// q0 = RN(x y) is within one ulp of x / n, r = x - q0 n is exact (FMA), and
+// RN(q0 + r y) is the correctly rounded quotient (P. Markstein, IBM J. Res.
+// Dev. 34(1), 1990).  The theorem needs a normal quotient, so dividends near
+// the underflow range take the IEEE division.
+__device__ __forceinline__ double div_int(double x, double n, double y) {
+  if (fabs(x) < 0x1p-900) return __ddiv_rn(x, n);
+  const double q0 = __dmul_rn(x, y);
+  const double r = __fma_rn(-q0, n, x);
+  return __fma_rn(r, y, q0);
+}
+
+// Correlation::iterate with step_k = 1 (walk.hpp:309-366) followed by the stop
+// test of walk.hpp:945-951 (step > min_L and R^2 < 0.999 or R < 0); returns
+// true when the walk stops after this token.
+__device__ __forceinline__ bool corr_step(Corr &c, uint32_t fi_u, const double *__restrict__ tab,
+                                          const double4 *s_ser, uint32_t step, uint32_t min_len) {
+  const double Sn = c.S;
+  const double Snp1 = __dadd_rn(Sn, 1.0);
+  const uint32_t S_u = (uint32_t)Sn;
+  const double t = (tab && S_u <= (uint32_t)kCorrTableS) ? __ldg(&tab[corr_tab_index(S_u, fi_u)])
+                                                         : corr_t(Sn, (double)fi_u);
+  double ES, DS, y;
+  if (S_u < kCorrSeries) {
+    const double4 q = s_ser[S_u];
+    ES = q.x;
+    DS = q.z;
+    y = q.w;
+  } else {
+    const double ES0 = S_u == kCorrSeries ? s_ser[kCorrSeries - 1].x : c.ES;
+    const double ESS0 = S_u == kCorrSeries ? s_ser[kCorrSeries - 1].y : c.ESS;
+    ES = __dadd_rn(ES0, __ddiv_rn(__dsub_rn(Snp1, ES0), Snp1));
+    const double ESS = __dadd_rn(ESS0, __ddiv_rn(__dsub_rn(__dmul_rn(Snp1, Snp1), ESS0), Snp1));
+    DS = __dsub_rn(ESS, __dmul_rn(ES, ES));
+    y = __drcp_rn(Snp1);
+    c.ES = ES;
+    c.ESS = ESS;
+  }
+  const double H1 = div_int(__dsub_rn(__dmul_rn(Sn, c.H), t), Snp1, y);
+  // N + 1 == S + 1
+  const double EH = __dadd_rn(c.EH, div_int(__dsub_rn(H1, c.EH), Snp1, y));
+  const double EHS = __dadd_rn(c.EHS, div_int(__dsub_rn(__dmul_rn(H1, Snp1), c.EHS), Snp1, y));
+  const double EHH = __dadd_rn(c.EHH, div_int(__dsub_rn(__dmul_rn(H1, H1), c.EHH), Snp1, y));
+  c.H = H1; c.EH = EH; c.EHS = EHS; c.EHH = EHH; c.S = Snp1;
+  if (step <= min_len) return false;
+  const double DH = __dsub_rn(EHH, __dmul_rn(EH, EH));
+  const double ex = __dsub_rn(EHS, __dmul_rn(EH, ES));
+  const double R = ex == 0.0 ? 0.0 : __ddiv_rn(ex, __dsqrt_rn(__dmul_rn(DH, DS)));
+  return __dmul_rn(R, R) < 0.999 || R < 0.0;
+}
+
+// The trace test of walk.hpp:997-1019: tanh(p_accept) <= p with
+// p_accept = (1 / (deg_s - cn)) * max(deg_s, deg_d) / min(deg_s, deg_d).
+__device__ __forceinline__ bool trace_test(int sd, int cn, int mx, int mn, double p) {
+  const int dn = sd - cn;
+  if (mx < (1 << 24) && dn < (1 << 24) && dn > -(1 << 24)) {
+    const float tf = tanhf((1.0f / (float)dn) * (float)mx / (float)mn);
+    const float pf = (float)p;
+    if (fabsf(tf - pf) > 0x1p-16f) return tf < pf;
+  }
+  const double p_accept = __ddiv_rn(__dmul_rn(__ddiv_rn(1.0, (double)dn), (double)mx), (double)mn);
+  return tanh(p_accept) <= p;
 }
 
 __device__ __forceinline__ uint64_t bloom_bit(uint32_t v) { return 1ULL << ((v * 0x9E3779B1u) >> 26); }
@@ -134,11 +204,24 @@ __device__ __forceinline__ uint32_t count_in_path(const uint32_t *p, uint32_t n,
   return c;
 }
 
+constexpr uint32_t kWalkThreads = 256;  // block size of k_walk
+constexpr uint32_t kSmemPath = 32;      // leading tokens of each walk kept in shared memory
+
 struct PathBuf {
   uint32_t *p;    // token storage of this walk
   uint32_t len;
   uint32_t cap;
+  uint32_t *s;    // this lane's column of the block's shared token rows
 };
+
+// Occurrences of v in the walk so far: the shared-memory rows, then the tail.
+__device__ __forceinline__ uint32_t count_in_walk(const PathBuf &pb, uint32_t v) {
+  const uint32_t m = pb.len < kSmemPath ? pb.len : kSmemPath;
+  uint32_t c = 0;
+  for (uint32_t i = 0; i < m; i++) c += pb.s[i * kWalkThreads] == v;
+  if (pb.len > kSmemPath) c += count_in_path(pb.p + kSmemPath, pb.len - kSmemPath, v);
+  return c;
+}
 
 // Append one token, moving the walk to a larger spill chunk when full.
 __device__ __forceinline__ bool path_push(const WalkArgs &a, PathBuf &pb, uint32_t v) {
@@ -154,6 +237,7 @@ __device__ __forceinline__ bool path_push(const WalkArgs &a, PathBuf &pb, uint32
     pb.p = np;
     pb.cap = ncap;
   }
+  if (pb.len < kSmemPath) pb.s[pb.len * kWalkThreads] = v;
   pb.p[pb.len++] = v;
   atomicAdd(&a.visit_freq[v], 1u);
   return true;
@@ -161,17 +245,26 @@ __device__ __forceinline__ bool path_push(const WalkArgs &a, PathBuf &pb, uint32
 
 // INJ: parity mode with injected draws; WEIGHTED: alias-table candidates.
 template <bool INJ, bool WEIGHTED>
-__global__ void __launch_bounds__(256, 3) k_walk(WalkArgs a) {
+__global__ void __launch_bounds__(kWalkThreads, 3) k_walk(WalkArgs a) {
+  __shared__ uint32_t s_path[kSmemPath * kWalkThreads];
+  __shared__ double4 s_ser[kCorrSeries];
+  for (uint32_t i = threadIdx.x; i < kCorrSeries; i += kWalkThreads) s_ser[i] = a.corr_series[i];
+  __syncthreads();
   unsigned long long my_tok = 0, my_tr = 0, my_it = 0, my_long = 0;
-  // walkers are claimed through kWalkClaimers counters so that claims do not
-  // serialize on one address
-  const uint32_t claimer = (blockIdx.x * blockDim.x + threadIdx.x) % kWalkClaimers;
+  const uint32_t lane = threadIdx.x & 31;
   for (;;) {
-    const uint32_t k = claimer + kWalkClaimers * atomicAdd(&a.next_walker[claimer], 1u);
-    if (k >= a.n_active) break;
+    // the whole warp claims walkers base .. base + 31; once base is past the
+    // end every lane leaves together
+    __syncwarp();
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(a.next_walker, 32u);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (base >= a.n_active) break;
+    const uint32_t k = base + lane;
+    if (k >= a.n_active) continue;
     const uint32_t w = a.active[k];
     const uint32_t start = w % a.v_num, replica = w / a.v_num;
-    PathBuf pb{a.arena + (uint64_t)k * a.slot_len, 0, a.slot_len};
+    PathBuf pb{a.arena + (uint64_t)k * a.slot_len, 0, a.slot_len, s_path + threadIdx.x};
     bool ok = path_push(a, pb, start);
     Corr c;
     corr_init(c);
@@ -233,26 +326,24 @@ __global__ void __launch_bounds__(256, 3) k_walk(WalkArgs a) {
       const uint32_t dd = (uint32_t)(a.row_ptr[dst + 1] - bd);
       const int sd = (int)deg, ddi = (int)dd;
       const int mx = sd > ddi ? sd : ddi, mn = sd < ddi ? sd : ddi;
-      const double p_accept = __ddiv_rn(__dmul_rn(__ddiv_rn(1.0, (double)(sd - cn)), (double)mx), (double)mn);
-      const bool trace = tanh(p_accept) <= p;
+      const bool trace = trace_test(sd, cn, mx, mn, p);
       my_tr += trace;
       // forward token
       step++;
       uint32_t fi;
       if (dst == cur) fi = cnt_cur;
-      else if (bloom & bloom_bit(dst)) fi = count_in_path(pb.p, pb.len, dst);
+      else if (bloom & bloom_bit(dst)) fi = count_in_walk(pb, dst);
       else fi = 0;
       if (!path_push(a, pb, dst)) { ok = false; break; }
       bloom |= bloom_bit(dst);
       if (dst == cur) cnt_cur++;
-      corr_iterate(c, fi, a.corr_tab);
-      if (corr_stop(c, step, a.min_len)) break;
+      if (corr_step(c, fi, a.corr_tab, s_ser, step, a.min_len)) break;
       if (trace) {
         step++;
         if (!path_push(a, pb, cur)) { ok = false; break; }
-        corr_iterate(c, cnt_cur, a.corr_tab);
+        const bool stop = corr_step(c, cnt_cur, a.corr_tab, s_ser, step, a.min_len);
         cnt_cur++;
-        if (corr_stop(c, step, a.min_len)) break;
+        if (stop) break;
       } else {
         if (dst != cur) cnt_cur = fi + 1;
         cur = dst;
@@ -266,10 +357,19 @@ __global__ void __launch_bounds__(256, 3) k_walk(WalkArgs a) {
     a.sent_ptr[k] = (uint64_t)(pb.p - a.arena);
     a.sent_len[k] = pb.len;
   }
-  atomicAdd(&a.stats[0], my_tok);
-  atomicAdd(&a.stats[1], my_tr);
-  atomicAdd(&a.stats[2], my_it);
-  atomicAdd(&a.stats[3], my_long);
+  __syncwarp();
+  for (int o = 16; o > 0; o >>= 1) {
+    my_tok += __shfl_down_sync(0xffffffffu, my_tok, o);
+    my_tr += __shfl_down_sync(0xffffffffu, my_tr, o);
+    my_it += __shfl_down_sync(0xffffffffu, my_it, o);
+    my_long += __shfl_down_sync(0xffffffffu, my_long, o);
+  }
+  if (lane == 0) {
+    if (my_tok) atomicAdd(&a.stats[0], my_tok);
+    if (my_tr) atomicAdd(&a.stats[1], my_tr);
+    if (my_it) atomicAdd(&a.stats[2], my_it);
+    if (my_long) atomicAdd(&a.stats[3], my_long);
+  }
 }
 
 }  // namespace felog
