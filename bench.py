@@ -199,6 +199,7 @@ def run_round(f, r, min_rounds, counters):
     counters["pairs"] += ts["pairs"]
     counters["kept"] += ts["kept_words"]
     counters["walk_ms"] += ws["ms"]
+    counters["last_walk"] = (ws["n_tokens"], ws["ms"])
     counters["train_ms"] += ts["ms_train"]
     counters["plan_ms"] += ts["ms_plan"]
     if r + 1 >= min_rounds:
@@ -324,6 +325,12 @@ def bench_mine(args):
         f.timer_mark(1)
         ms = f.timer_elapsed()
     launches = f.kernel_launches() - launches0
+    # the walker against the attainable rate of its own access pattern: the
+    # memory skeleton of the last timed round (same walkers and lengths,
+    # dependent uniform-neighbour gathers, no arithmetic), timed outside the
+    # timed region
+    ceil_ms, ceil_tok = f.walk_ceiling()
+    last_tok, last_ms = cnt["last_walk"]
     ms_max = max_over_ranks(pg, ms)
     tokens_all = sum_over_ranks(pg, cnt["tokens"])
     value = tokens_all / (ms_max * 1e-3)
@@ -408,7 +415,12 @@ def bench_mine(args):
                      "unit": "GB/s", "frac": sg_achieved / peak,
                      "peak_source": peak_kind,
                      "walk_kernel": {"achieved": walk_achieved, "frac": walk_achieved / peak,
-                                     "bytes_per_step": WALK_BYTES_PER_STEP}},
+                                     "bytes_per_step": WALK_BYTES_PER_STEP,
+                                     "gather_ceiling": {"steps_per_s": ceil_tok / (ceil_ms * 1e-3),
+                                                        "walk_steps_per_s": last_tok / (last_ms * 1e-3),
+                                                        "frac": (last_tok / last_ms) / (ceil_tok / ceil_ms),
+                                                        "what": "felog_walk_ceiling: memory skeleton of the "
+                                                                "last timed round on the same CSR"}}},
         "e2e": {"value": e2e_value, "unit": "tokens/s", "h2d_bytes_per_step": int(V),
                 "d2h_bytes_per_step": int(vs * 128 * 4 + V), "ms_per_step": e2e_ms / args.steps,
                 "tokens_per_step": e2e["tokens"] / args.steps},

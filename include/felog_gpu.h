@@ -222,6 +222,13 @@ felog_status felog_get_corpus(felog_ctx *ctx, uint32_t *tokens, uint64_t tok_cap
 felog_status felog_set_corpus(felog_ctx *ctx, const uint32_t *tokens, const uint64_t *sent_off,
                               uint64_t n_sentences);
 felog_status felog_get_visit_freq(felog_ctx *ctx, uint64_t *freq);
+/* Attainable-rate ceiling of the last walk round (no reference counterpart):
+ * a memory skeleton of that round on the loaded CSR - the same walkers and
+ * tokens per walker, the same launch shape, dependent uniform-neighbour
+ * gathers at the round's forward-step rate, no arithmetic - timed on the
+ * device (best of 3).  ms: its duration; tokens: the tokens it emits.  The
+ * corpus is left unchanged. */
+felog_status felog_walk_ceiling(felog_ctx *ctx, float *ms, uint64_t *tokens);
 
 /* ---- trainer ---- */
 /* Vocabulary, unigram table and InitNet rows (word2vec.cu:834-902); also starts a new

@@ -94,6 +94,7 @@ struct felog_ctx {
   DevBuf<uint64_t> sent_ptr;
   DevBuf<uint32_t> sent_len;
   uint64_t n_sent = 0, n_tok = 0;
+  uint64_t last_walk_tokens = 0, last_walk_traces = 0;  // totals of the last walk round
   bool corpus_ready = false;
   DevBuf<unsigned int> visit_freq;
   uint64_t words_sum_cum = 0;
@@ -724,6 +725,8 @@ extern "C" felog_status felog_walk_round(felog_ctx *c, uint32_t round, const fel
   CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1), "walk_round");
   c->n_sent = na;
   c->n_tok = h[0];
+  c->last_walk_tokens = h[0];
+  c->last_walk_traces = h[1];
   c->corpus_ready = true;
   s = budget_records(c);
   if (s != FELOG_OK) return s;
@@ -747,6 +750,49 @@ extern "C" felog_status felog_walk_round(felog_ctx *c, uint32_t round, const fel
     if (s != FELOG_OK) return s;
   }
   return FELOG_OK;
+}
+
+namespace {
+felog_status walk_ceiling_run(felog_ctx *c, DevBuf<uint32_t> &scratch, float *ms) {
+  // forward steps per token of the last round: every token but the start and
+  // the return tokens of traces came from a gather
+  const double fwd = (double)(c->last_walk_tokens - c->n_sent - c->last_walk_traces) / (double)c->last_walk_tokens;
+  const uint32_t frac = (uint32_t)std::min(4294967295.0, std::max(0.0, fwd) * 4294967296.0);
+  CK(scratch.ensure(c->arena_cap), "walk_ceiling: scratch");
+  CK(c->walk_claim.ensure(1), "walk_ceiling");
+  int per_sm = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_walk_skeleton, kWalkThreads, 0), "walk_ceiling");
+  const int blocks = c->sm_count * std::max(per_sm, 1);
+  float best = 0;
+  for (int rep = 0; rep < 3; rep++) {
+    CK(cudaMemsetAsync(c->walk_claim.p, 0, 4, c->stream), "walk_ceiling");
+    CK(cudaEventRecord(c->ev0, c->stream), "walk_ceiling");
+    k_walk_skeleton<<<blocks, kWalkThreads, 0, c->stream>>>(c->row_ptr.p, c->adj.p, c->V, (uint32_t)c->n_sent,
+                                                             c->active.p, c->sent_ptr.p, c->sent_len.p, frac,
+                                                             scratch.p, c->walk_claim.p);
+    c->launches++;
+    CK(cudaGetLastError(), "walk_ceiling");
+    CK(cudaEventRecord(c->ev1, c->stream), "walk_ceiling");
+    CK(cudaEventSynchronize(c->ev1), "walk_ceiling");
+    float t = 0;
+    CK(cudaEventElapsedTime(&t, c->ev0, c->ev1), "walk_ceiling");
+    if (rep == 0 || t < best) best = t;
+  }
+  *ms = best;
+  return FELOG_OK;
+}
+}  // namespace
+
+extern "C" felog_status felog_walk_ceiling(felog_ctx *c, float *ms, uint64_t *tokens) {
+  if (!c || !ms) return FELOG_INVALID_ARG;
+  if (!c->corpus_ready || !c->n_sent || !c->last_walk_tokens)
+    return fail(c, FELOG_NOT_READY, "walk_ceiling: run a walk round first");
+  CK(cudaSetDevice(c->device), "walk_ceiling");
+  DevBuf<uint32_t> scratch;
+  const felog_status s = walk_ceiling_run(c, scratch, ms);
+  scratch.release();
+  if (s == FELOG_OK && tokens) *tokens = c->last_walk_tokens;
+  return s;
 }
 
 extern "C" felog_status felog_corpus_size(felog_ctx *c, uint64_t *n_sentences, uint64_t *n_tokens) {
@@ -808,6 +854,7 @@ extern "C" felog_status felog_set_corpus(felog_ctx *c, const uint32_t *tokens, c
   }
   c->arena_cap = std::max<uint64_t>(ntok, 4);
   c->n_sent = n_sentences;
+  c->last_walk_tokens = 0;  // no walk round behind this corpus
   c->n_tok = ntok;
   c->corpus_ready = true;
   return FELOG_OK;

@@ -372,4 +372,47 @@ __global__ void __launch_bounds__(kWalkThreads, 3) k_walk(WalkArgs a) {
   }
 }
 
+// Memory skeleton of a finished walk round, for its attainable-rate ceiling:
+// every walker of the round emits as many tokens as its walk had; a token is
+// a dependent uniform-neighbour gather (the candidate's adjacency entry, then
+// the neighbour's row_ptr pair) with probability gather_frac (the round's
+// forward steps per token), else a repeat of the current vertex (the return
+// token of a trace, which loads nothing).  Same block size, residency and
+// warp claims as k_walk; no FP64, no trace test, no revisit counts and no
+// visit counters.  Tokens go to a scratch buffer at the walk's offsets.
+__global__ void __launch_bounds__(kWalkThreads, 3)
+    k_walk_skeleton(const uint64_t *__restrict__ row_ptr, const uint2 *__restrict__ adj, uint32_t v_num,
+                    uint32_t n_active, const uint32_t *__restrict__ active, const uint64_t *__restrict__ sent_ptr,
+                    const uint32_t *__restrict__ sent_len, uint32_t gather_frac, uint32_t *out,
+                    unsigned int *next_walker) {
+  const uint32_t lane = threadIdx.x & 31;
+  for (;;) {
+    __syncwarp();
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(next_walker, 32u);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (base >= n_active) break;
+    const uint32_t k = base + lane;
+    if (k >= n_active) continue;
+    uint32_t cur = active[k] % v_num;
+    uint64_t b = row_ptr[cur];
+    uint32_t deg = (uint32_t)(row_ptr[cur + 1] - b);
+    uint32_t *o = out + sent_ptr[k];
+    const uint32_t len = sent_len[k];
+    if (len) o[0] = cur;
+    uint32_t h = k * 0x9E3779B1u;
+    for (uint32_t t = 1; t < len; t++) {
+      h = h * 1664525u + 1013904223u;
+      if (deg && (h >> 8) < (gather_frac >> 8)) {
+        const uint32_t r = (uint32_t)(((uint64_t)(h ^ (h >> 13)) * deg) >> 32);
+        const uint32_t dst = adj[b + r].x;
+        b = row_ptr[dst];
+        deg = (uint32_t)(row_ptr[dst + 1] - b);
+        cur = dst;
+      }
+      o[t] = cur;
+    }
+  }
+}
+
 }  // namespace felog

@@ -142,6 +142,7 @@ def gpu_lib():
         L.felog_get_corpus.argtypes = [_P, _P, ctypes.c_uint64, _P, ctypes.c_uint64]
         L.felog_set_corpus.argtypes = [_P, _P, _P, ctypes.c_uint64]
         L.felog_get_visit_freq.argtypes = [_P, _P]
+        L.felog_walk_ceiling.argtypes = [_P, _P, _P]
         L.felog_init_model.argtypes = [_P]
         L.felog_vocab_info.argtypes = [_P, _P, _P]
         L.felog_get_vocab.argtypes = [_P, _P, _P]
@@ -306,6 +307,14 @@ class Felog:
         self._ck(self._L.felog_walk_round(self.h, round_, ctypes.byref(dr) if dr is not None else None,
                                           ctypes.byref(st)))
         return _struct_dict(st)
+
+    def walk_ceiling(self):
+        """Memory skeleton of the last walk round (felog_walk_ceiling):
+        returns (ms, tokens), the skeleton's device time and token count."""
+        ms = ctypes.c_float()
+        tok = ctypes.c_uint64()
+        self._ck(self._L.felog_walk_ceiling(self.h, ctypes.byref(ms), ctypes.byref(tok)))
+        return ms.value, tok.value
 
     def corpus(self):
         ns = ctypes.c_uint64()

@@ -196,3 +196,21 @@ def test_bad_vertex_is_an_error():
     with pytest.raises(fb.FelogError) as ei:
         f.load_graph(e, 3)
     assert ei.value.status == 1
+
+
+def test_walk_ceiling_skeleton_leaves_corpus():
+    """felog_walk_ceiling times a memory skeleton of the last round (same walkers
+    and token counts) without touching the round's corpus."""
+    g = fb.synth_graph(seed=5, v_target=8192, e_target=65536, holdout=0.0)
+    V = g["v_num"]
+    f = fb.Felog(v_num=V, seed=9)
+    f.load_graph(g["edges"], V)
+    with pytest.raises(fb.FelogError):
+        f.walk_ceiling()  # no walk round yet
+    ws = f.walk_round(0)
+    tok0, off0 = f.corpus()
+    ms, tokens = f.walk_ceiling()
+    assert ms > 0 and tokens == ws["n_tokens"]
+    tok1, off1 = f.corpus()
+    assert np.array_equal(tok0, tok1) and np.array_equal(off0, off1)
+    f.close()
