@@ -490,6 +490,52 @@ def bench_reference(args):
     print(json.dumps(out), flush=True)
 
 
+def bench_gcn(args):
+    """Common neighbours per edge (the reference's offline gcn tool) on the
+    configuration's training edges: device time of felog_common_neighbours
+    (warm-up calls, then the best of the timed calls), the same call end to end
+    with host arrays, and the oracle (the tool restated in C, one thread) on
+    the same edges as the CPU baseline.  One JSON line."""
+    import felog_b200 as fb
+    cfg = CONFIGS[args.config]
+    g = make_graph(cfg)
+    V = g["v_num"]
+    src = np.ascontiguousarray(g["edges"]["src"], np.uint32)
+    dst = np.ascontiguousarray(g["edges"]["dst"], np.uint32)
+    n = len(src)
+    f = fb.Felog(v_num=V, seed=1)
+    for _ in range(args.warmup):
+        cn, _ = f.common_neighbours(src, dst, V, True)
+    dev, wall = [], []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        cn, ms = f.common_neighbours(src, dst, V, True)
+        wall.append(time.perf_counter() - t0)
+        dev.append(ms)
+    launches = f.kernel_launches()
+    f.close()
+    out = {"metric": "common-neighbour edges/s (gcn tool, undirected)", "value": n / (min(dev) * 1e-3),
+           "unit": "edges/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": min(dev), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": "u32 ids, i32 counts", "data": "synthetic (seeded R-MAT, see config)",
+           "config": {"workload": f"gcn tool on the training edges of the seed-{cfg['seed']} R-MAT "
+                                  f"({cfg['v_target']:,} vertex ids / {cfg['e_target']:,} undirected edges)",
+                      "v_num": V, "edges": n,
+                      "sum_cn": int(cn.astype(np.int64).sum()), "max_degree": g["info"]["max_degree"]},
+           "e2e": {"value": n / min(wall), "unit": "edges/s", "h2d_bytes_per_step": 8 * n,
+                   "d2h_bytes_per_step": 4 * n}, "gpu_launches_total": int(launches)}
+    if not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        import oracle_binding as ob
+        t0 = time.perf_counter()
+        ref = ob.common_neighbours(src, dst, V, True)
+        t = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": n / t, "unit": "edges/s", "cores": 1, "kind": "port",
+                               "sample": f"oracle on all {n} edges, {t:.1f}s, 1 thread"}
+        out["parity_vs_oracle"] = bool(np.array_equal(ref, cn))
+    print(json.dumps(out), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -505,8 +551,12 @@ def main():
     ap.add_argument("--no-forms", action="store_true", help="skip the end-to-end plain vs learned comparison")
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the default launch shape (profiling: a tuner timed under ncu is distorted)")
+    ap.add_argument("--workload", default="walk-sgns", choices=["walk-sgns", "gcn"],
+                    help="gcn: the offline common-neighbour tool instead of the walk + SGNS rounds")
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.workload == "gcn":
+        bench_gcn(args)
+    elif args.impl == "reference":
         bench_reference(args)
     else:
         bench_mine(args)

@@ -230,6 +230,20 @@ felog_status felog_get_visit_freq(felog_ctx *ctx, uint64_t *freq);
  * corpus is left unchanged. */
 felog_status felog_walk_ceiling(felog_ctx *ctx, float *ms, uint64_t *tokens);
 
+/* ---- offline edge data ---- */
+/* Common neighbours per input edge: the reference's offline tool
+ * (src/tools/gcn.cpp:248-357; its CLI is gcn -i -o -v -t -s --make-undirected).
+ * src/dst: n input edges (host memory); undirected != 0 doubles them as the
+ * tool's --make-undirected does.  cn[e] (host, n entries): the number of
+ * common neighbours of src[e] and dst[e] as the tool counts them (repeats and
+ * src/dst themselves taken out by its rule; every edge of an unordered pair
+ * reports the count of the pair's first edge).  ms (may be NULL): device time
+ * of the computation, host copies excluded.  Needs no loaded graph.
+ * FELOG_INVALID_ARG on a vertex id >= v_num or more than 2^31 - 1 adjacency
+ * entries. */
+felog_status felog_common_neighbours(felog_ctx *ctx, const uint32_t *src, const uint32_t *dst, uint64_t n,
+                                     uint32_t v_num, int undirected, int32_t *cn, float *ms);
+
 /* ---- trainer ---- */
 /* Vocabulary, unigram table and InitNet rows (word2vec.cu:834-902); also starts a new
  * training run: stop flags, visit counts and the budget records are cleared. */

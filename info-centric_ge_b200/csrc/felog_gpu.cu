@@ -19,6 +19,7 @@
 
 #include "budget.cuh"
 #include "common.cuh"
+#include "gcn.cuh"
 #include "graph.cuh"
 #include "mlp.cuh"
 #include "pairs.cuh"
@@ -792,6 +793,117 @@ extern "C" felog_status felog_walk_ceiling(felog_ctx *c, float *ms, uint64_t *to
   const felog_status s = walk_ceiling_run(c, scratch, ms);
   scratch.release();
   if (s == FELOG_OK && tokens) *tokens = c->last_walk_tokens;
+  return s;
+}
+
+namespace {
+struct GcnBufs {
+  DevBuf<uint32_t> src, dst, nbr, heavy, idx, idx_alt;
+  DevBuf<unsigned long long> keys, keys_alt, pkeys, pkeys_alt, n_heavy;
+  DevBuf<uint64_t> row_ptr, head, head_scan;
+  DevBuf<int32_t> cn_own, cn_out;
+  DevBuf<unsigned char> tmp;
+  void release() {
+    src.release(); dst.release(); nbr.release(); heavy.release(); idx.release(); idx_alt.release();
+    keys.release(); keys_alt.release(); pkeys.release(); pkeys_alt.release(); n_heavy.release();
+    row_ptr.release(); head.release(); head_scan.release(); cn_own.release(); cn_out.release(); tmp.release();
+  }
+};
+
+int key_bits(uint32_t v_num) {
+  int b = 1;
+  while (b < 32 && (1ULL << b) < (uint64_t)v_num) b++;
+  return 32 + b;
+}
+
+felog_status gcn_run(felog_ctx *c, GcnBufs &B, const uint32_t *src, const uint32_t *dst, uint64_t n, uint32_t v_num,
+                     int undirected, int32_t *cn, float *ms) {
+  const uint64_t m = undirected ? 2 * n : n;
+  CK(B.src.ensure(n), "common_neighbours");
+  CK(B.dst.ensure(n), "common_neighbours");
+  CK(B.keys.ensure(m), "common_neighbours");
+  CK(B.keys_alt.ensure(m), "common_neighbours");
+  CK(B.nbr.ensure(m), "common_neighbours");
+  CK(B.row_ptr.ensure((size_t)v_num + 1), "common_neighbours");
+  CK(B.cn_own.ensure(n), "common_neighbours");
+  CK(B.cn_out.ensure(n), "common_neighbours");
+  CK(B.heavy.ensure(n), "common_neighbours");
+  CK(B.n_heavy.ensure(1), "common_neighbours");
+  CK(B.pkeys.ensure(n), "common_neighbours");
+  CK(B.pkeys_alt.ensure(n), "common_neighbours");
+  CK(B.idx.ensure(n), "common_neighbours");
+  CK(B.idx_alt.ensure(n), "common_neighbours");
+  CK(B.head.ensure(n), "common_neighbours");
+  CK(B.head_scan.ensure(n), "common_neighbours");
+  CK(cudaMemcpyAsync(B.src.p, src, 4 * n, cudaMemcpyHostToDevice, c->stream), "common_neighbours");
+  CK(cudaMemcpyAsync(B.dst.p, dst, 4 * n, cudaMemcpyHostToDevice, c->stream), "common_neighbours");
+  CK(cudaMemsetAsync(c->derr.p, 0, sizeof(int), c->stream), "common_neighbours");
+  CK(cudaMemsetAsync(B.n_heavy.p, 0, 8, c->stream), "common_neighbours");
+  CK(cudaEventRecord(c->ev0, c->stream), "common_neighbours");
+  const int kb = key_bits(v_num);
+  k_gcn_keys<<<grid_for(c, n, 256), 256, 0, c->stream>>>(B.src.p, B.dst.p, n, v_num, undirected, B.keys.p, c->derr.p);
+  c->launches++;
+  // rows sorted by neighbour: one radix sort of (src << 32 | dst)
+  cub::DoubleBuffer<unsigned long long> kd(B.keys.p, B.keys_alt.p);
+  size_t tb = 0;
+  CK(cub::DeviceRadixSort::SortKeys(nullptr, tb, kd, (int)m, 0, kb, c->stream), "common_neighbours: sort");
+  CK(B.tmp.ensure(tb), "common_neighbours");
+  CK(cub::DeviceRadixSort::SortKeys(B.tmp.p, tb, kd, (int)m, 0, kb, c->stream), "common_neighbours: sort");
+  k_gcn_rows<<<grid_for(c, std::max<uint64_t>(m, 1), 256), 256, 0, c->stream>>>(kd.Current(), m, v_num, B.row_ptr.p,
+                                                                                B.nbr.p);
+  c->launches++;
+  k_gcn_edges<<<grid_for(c, n, 256), 256, 0, c->stream>>>(B.src.p, B.dst.p, n, B.row_ptr.p, B.nbr.p, B.cn_own.p,
+                                                          B.heavy.p, B.n_heavy.p);
+  c->launches++;
+  k_gcn_heavy<<<c->sm_count * 8, 256, 0, c->stream>>>(B.src.p, B.dst.p, B.heavy.p, B.n_heavy.p, B.row_ptr.p, B.nbr.p,
+                                                      B.cn_own.p);
+  c->launches++;
+  // every edge of an unordered pair takes the count of the pair's first edge
+  k_gcn_pair_keys<<<grid_for(c, n, 256), 256, 0, c->stream>>>(B.src.p, B.dst.p, n, B.pkeys.p, B.idx.p);
+  c->launches++;
+  cub::DoubleBuffer<unsigned long long> pk(B.pkeys.p, B.pkeys_alt.p);
+  cub::DoubleBuffer<uint32_t> pv(B.idx.p, B.idx_alt.p);
+  tb = 0;
+  CK(cub::DeviceRadixSort::SortPairs(nullptr, tb, pk, pv, (int)n, 0, kb, c->stream), "common_neighbours: sort");
+  CK(B.tmp.ensure(tb), "common_neighbours");
+  CK(cub::DeviceRadixSort::SortPairs(B.tmp.p, tb, pk, pv, (int)n, 0, kb, c->stream), "common_neighbours: sort");
+  k_gcn_heads<<<grid_for(c, n, 256), 256, 0, c->stream>>>(pk.Current(), n, B.head.p);
+  c->launches++;
+  tb = 0;
+  CK(cub::DeviceScan::InclusiveScan(nullptr, tb, B.head.p, B.head_scan.p, GcnMax(), (int)n, c->stream),
+     "common_neighbours: scan");
+  CK(B.tmp.ensure(tb), "common_neighbours");
+  CK(cub::DeviceScan::InclusiveScan(B.tmp.p, tb, B.head.p, B.head_scan.p, GcnMax(), (int)n, c->stream),
+     "common_neighbours: scan");
+  k_gcn_scatter<<<grid_for(c, n, 256), 256, 0, c->stream>>>(pv.Current(), B.head_scan.p, n, B.cn_own.p, B.cn_out.p);
+  c->launches++;
+  CK(cudaGetLastError(), "common_neighbours");
+  CK(cudaEventRecord(c->ev1, c->stream), "common_neighbours");
+  felog_status s = check_dev_err(c, "common_neighbours");
+  if (s != FELOG_OK) return s;
+  CK(cudaMemcpyAsync(cn, B.cn_out.p, 4 * n, cudaMemcpyDeviceToHost, c->stream), "common_neighbours");
+  CK(cudaStreamSynchronize(c->stream), "common_neighbours");
+  if (ms) CK(cudaEventElapsedTime(ms, c->ev0, c->ev1), "common_neighbours");
+  return FELOG_OK;
+}
+}  // namespace
+
+extern "C" felog_status felog_common_neighbours(felog_ctx *c, const uint32_t *src, const uint32_t *dst, uint64_t n,
+                                                uint32_t v_num, int undirected, int32_t *cn, float *ms) {
+  if (!c || (n && (!src || !dst || !cn))) return FELOG_INVALID_ARG;
+  if ((undirected ? 2 * n : n) >= (1ULL << 31))
+    return fail(c, FELOG_INVALID_ARG, "common_neighbours: at most 2^31 - 1 adjacency entries");
+  if (ms) *ms = 0;
+  if (n == 0) return FELOG_OK;
+  // ids are checked here: the device passes index rows with them
+  for (uint64_t e = 0; e < n; e++)
+    if (src[e] >= v_num || dst[e] >= v_num)
+      return fail(c, FELOG_INVALID_ARG, "common_neighbours: edge %llu has an endpoint >= v_num",
+                  (unsigned long long)e);
+  CK(cudaSetDevice(c->device), "common_neighbours");
+  GcnBufs B;
+  const felog_status s = gcn_run(c, B, src, dst, n, v_num, undirected, cn, ms);
+  B.release();
   return s;
 }
 

@@ -143,6 +143,7 @@ def gpu_lib():
         L.felog_set_corpus.argtypes = [_P, _P, _P, ctypes.c_uint64]
         L.felog_get_visit_freq.argtypes = [_P, _P]
         L.felog_walk_ceiling.argtypes = [_P, _P, _P]
+        L.felog_common_neighbours.argtypes = [_P, _P, _P, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_int, _P, _P]
         L.felog_init_model.argtypes = [_P]
         L.felog_vocab_info.argtypes = [_P, _P, _P]
         L.felog_get_vocab.argtypes = [_P, _P, _P]
@@ -307,6 +308,17 @@ class Felog:
         self._ck(self._L.felog_walk_round(self.h, round_, ctypes.byref(dr) if dr is not None else None,
                                           ctypes.byref(st)))
         return _struct_dict(st)
+
+    def common_neighbours(self, src, dst, v_num, undirected=True):
+        """felog_common_neighbours: per input edge, the common-neighbour count
+        of the reference's gcn tool.  Returns (cn int32 array, device ms)."""
+        src = np.ascontiguousarray(src, np.uint32)
+        dst = np.ascontiguousarray(dst, np.uint32)
+        cn = np.zeros(len(src), np.int32)
+        ms = ctypes.c_float()
+        self._ck(self._L.felog_common_neighbours(self.h, _addr(src), _addr(dst), len(src), v_num, int(undirected),
+                                                 _addr(cn), ctypes.byref(ms)))
+        return cn, ms.value
 
     def walk_ceiling(self):
         """Memory skeleton of the last walk round (felog_walk_ceiling):

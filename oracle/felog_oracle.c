@@ -1134,3 +1134,118 @@ double orc_mlp_loss_grad(const float *params, const float *X, const uint8_t *cou
   for (int i = 0; i < MLP_P; i++) grad[i] /= (double)n;
   return loss / (double)n;
 }
+
+/* ------------------------------------------------------------------------
+ * Common neighbours (src/tools/gcn.cpp) */
+
+static int cmp_u32(const void *a, const void *b) {
+  const uint32_t x = *(const uint32_t *)a, y = *(const uint32_t *)b;
+  return x < y ? -1 : x > y;
+}
+
+/* first index of [lo, hi) with v[i] >= key (std::lower_bound) */
+static uint64_t lower_u32(const uint32_t *v, uint64_t lo, uint64_t hi, uint32_t key) {
+  while (lo < hi) {
+    const uint64_t mid = lo + (hi - lo) / 2;
+    if (v[mid] < key) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+
+/* myIntersectition (gcn.cpp:146-196): galloping search of each element of the
+ * shorter list (the second list on a size tie) in the longer one; a match
+ * appends the short element and keeps the long position, so repeated short
+ * elements match again.  Appends to out (capacity >= |short|), returns the
+ * count. */
+static uint32_t gcn_intersect(const uint32_t *v1, int n1, const uint32_t *v2, int n2, uint32_t *out) {
+  if (n1 == 0 || n2 == 0) return 0;
+  const uint32_t *lv = n1 > n2 ? v1 : v2, *sv = n1 > n2 ? v2 : v1;
+  const int nl = n1 > n2 ? n1 : n2, ns = n1 > n2 ? n2 : n1;
+  if (lv[nl - 1] < sv[0] || lv[0] > sv[ns - 1]) return 0;
+  uint32_t cnt = 0;
+  int p1 = 0, p2 = 0;
+  while (p1 < nl && p2 < ns) {
+    int step = 1, last = step;
+    if (sv[p2] < lv[p1]) {
+      p2++;
+      continue;
+    }
+    while (lv[p1 + step - 1] < sv[p2]) {
+      step *= 2;
+      last = p1 + step < nl ? step : nl - p1;
+      if (p1 + step >= nl) break;
+    }
+    if (lv[nl - 1] < sv[p2]) {
+      p2++;
+      break;
+    }
+    const int t = (int)lower_u32(lv, (uint64_t)(p1 + step / 2), (uint64_t)(p1 + last), sv[p2]);
+    if (lv[t] == sv[p2]) {
+      out[cnt++] = sv[p2];
+      p2++;
+      p1 = t;
+    } else {
+      p2++;
+      p1 = p1 + step / 2;
+    }
+  }
+  return cnt;
+}
+
+int orc_common_neighbours(const uint32_t *src, const uint32_t *dst, uint64_t n, uint32_t v_num, int undirected,
+                          int32_t *cn) {
+  for (uint64_t e = 0; e < n; e++)
+    if (src[e] >= v_num || dst[e] >= v_num) return -1;
+  const uint64_t m = undirected ? 2 * n : n;
+  uint64_t *rp = (uint64_t *)calloc((size_t)v_num + 1, sizeof(uint64_t));
+  uint32_t *nbr = (uint32_t *)malloc((size_t)(m ? m : 1) * sizeof(uint32_t));
+  int32_t *data = (int32_t *)malloc((size_t)(m ? m : 1) * sizeof(int32_t));
+  uint64_t *fill = (uint64_t *)malloc(((size_t)v_num + 1) * sizeof(uint64_t));
+  uint32_t *inter = NULL;
+  if (!rp || !nbr || !data || !fill) goto fail;
+  /* rows in input order, the doubled edge list interleaved (e, e^T) */
+  for (uint64_t e = 0; e < n; e++) {
+    rp[src[e] + 1]++;
+    if (undirected) rp[dst[e] + 1]++;
+  }
+  for (uint32_t v = 0; v < v_num; v++) rp[v + 1] += rp[v];
+  memcpy(fill, rp, ((size_t)v_num + 1) * sizeof(uint64_t));
+  for (uint64_t e = 0; e < n; e++) {
+    nbr[fill[src[e]]++] = dst[e];
+    if (undirected) nbr[fill[dst[e]]++] = src[e];
+  }
+  uint64_t maxdeg = 0;
+  for (uint32_t v = 0; v < v_num; v++) {
+    const uint64_t d = rp[v + 1] - rp[v];
+    if (d > 1) qsort(nbr + rp[v], (size_t)d, sizeof(uint32_t), cmp_u32);
+    if (d > maxdeg) maxdeg = d;
+  }
+  for (uint64_t i = 0; i < m; i++) data[i] = -1;
+  inter = (uint32_t *)malloc((size_t)(maxdeg ? maxdeg : 1) * sizeof(uint32_t));
+  if (!inter) goto fail;
+  for (uint64_t e = 0; e < n; e++) {
+    const uint32_t s = src[e], d = dst[e];
+    const uint64_t pos = lower_u32(nbr, rp[s], rp[s + 1], d);
+    if (data[pos] != -1) continue;
+    const uint32_t k = gcn_intersect(nbr + rp[s], (int)(rp[s + 1] - rp[s]), nbr + rp[d], (int)(rp[d + 1] - rp[d]), inter);
+    uint32_t c = k;
+    if (c > 0) {
+      if (inter[0] == s || inter[0] == d) c--;
+      if (c > 1)
+        for (uint32_t i = 1; i < k; i++) {
+          if (inter[i] == inter[i - 1]) c--;
+          else if (inter[i] == s || inter[i] == d) c--;
+        }
+    }
+    data[pos] = (int32_t)c;
+    const uint64_t mp = lower_u32(nbr, rp[d], rp[d + 1], s);
+    if (mp < rp[d + 1] && nbr[mp] == s) data[mp] = (int32_t)c;
+  }
+  for (uint64_t e = 0; e < n; e++) cn[e] = data[lower_u32(nbr, rp[src[e]], rp[src[e] + 1], dst[e])];
+  free(rp); free(nbr); free(data); free(fill); free(inter);
+  return 0;
+fail:
+  free(rp); free(nbr); free(data); free(fill); free(inter);
+  return -1;
+}

@@ -183,6 +183,18 @@ uint64_t orc_convergence(const float *syn0, const uint32_t *id2offset, int dim, 
 void orc_eval_choose(uint64_t seed, uint32_t round, uint32_t v, uint32_t deg, uint32_t *chosen /* 30 */);
 float orc_cosine(const float *a, const float *b, int dim);
 
+/* Common neighbours per input edge: the reference's offline tool
+ * (src/tools/gcn.cpp:248-357) with one thread.  The CSR holds the input
+ * edges (doubled in input order when undirected), each row sorted by
+ * neighbour; every input edge, in order, takes the first sorted entry of
+ * (src, dst) and, unless that entry already holds a count, intersects the
+ * two neighbour lists with the tool's galloping search and corrects the size
+ * for src/dst and repeats; the count goes to that entry and to the first entry
+ * of (dst, src).  cn[e] is the count held by the first (src, dst) entry.
+ * Returns 0, or -1 on a vertex id >= v_num or an allocation failure. */
+int orc_common_neighbours(const uint32_t *src, const uint32_t *dst, uint64_t n, uint32_t v_num, int undirected,
+                          int32_t *cn);
+
 #ifdef __cplusplus
 }
 #endif

@@ -6,13 +6,16 @@ reference's own output on seeded synthetic inputs:
 
   walk_*.npz   include/walk.hpp run by oracle/_ref/ref_walk with injected draws:
                the graph, per-walker draw streams and the per-round corpus.
+  gcn_*.npz    src/tools/gcn.cpp (the offline common-neighbour tool) run by
+               oracle/_ref/ref_gcn on text edge lists: per input edge its
+               common-neighbour count.
   plan_*.npz   src/word2vec.cu's ReadVocabFromDegree / InitNet /
                InitUnigramTable / TrainModelThreadMemory run by
                oracle/_ref/ref_sgns_plan: vocabulary order, subsampling
                thresholds, unigram table digest, syn0 head and the batch plan
                (sentence_length, sen, negSample per batch).
 
-Usage: python tests/golden/make_fixtures.py
+Usage: python tests/golden/make_fixtures.py [walk] [plan] [gcn]   (default: all)
 """
 import hashlib
 import os
@@ -183,7 +186,48 @@ def run_plan_fixture(name, deg, sents, recipe, dim, window, negative, sample, mi
           f"subsampled words={int((thr < 65535).sum()) if len(thr) else 0}")
 
 
+def run_gcn_fixture(name, src, dst, V, undirected):
+    with tempfile.TemporaryDirectory() as td:
+        ein, eout = os.path.join(td, "e.txt"), os.path.join(td, "o.txt")
+        with open(ein, "w") as fh:
+            fh.write("".join(f"{a} {b}\n" for a, b in zip(src.tolist(), dst.tolist())))
+        subprocess.run([os.path.join(REFBIN, "ref_gcn"), ein, eout, str(V), str(int(undirected))], check=True,
+                       stdout=subprocess.DEVNULL)
+        out = np.loadtxt(eout, dtype=np.int64, ndmin=2)
+    assert out.shape == (len(src), 3) and (out[:, 0] == src).all() and (out[:, 1] == dst).all()
+    np.savez_compressed(os.path.join(HERE, name), src=src.astype(np.uint32), dst=dst.astype(np.uint32),
+                        v_num=np.uint32(V), undirected=np.uint8(undirected), cn=out[:, 2].astype(np.int32))
+    print(name, len(src), "edges", flush=True)
+
+
+def gcn_fixtures():
+    rng = np.random.default_rng(2024)
+    # small multigraph: repeated edges, reciprocal pairs and self-loops
+    V = 64
+    a = rng.integers(0, V, 420)
+    b = (a + 1 + rng.zipf(1.6, 420) % (V - 1)) % V
+    src = np.concatenate([a, b[:40], a[:30], np.arange(0, V, 9)])
+    dst = np.concatenate([b, a[:40], b[:30], np.arange(0, V, 9)])
+    run_gcn_fixture("gcn_multi64_undirected.npz", src, dst, V, True)
+    # directed: every vertex also gets an out-edge so that no neighbour list is empty
+    ring = np.arange(V)
+    run_gcn_fixture("gcn_multi64_directed.npz", np.concatenate([src, ring]), np.concatenate([dst, (ring + 1) % V]),
+                    V, False)
+    # R-MAT graph with hubs (both lists long), plus reciprocal copies of 5% of its edges
+    g = fb.synth_graph(seed=4, v_target=4096, e_target=40000, holdout=0.0)
+    e = g["edges"]
+    k = len(e) // 20
+    src = np.concatenate([e["src"], e["dst"][:k]])
+    dst = np.concatenate([e["dst"], e["src"][:k]])
+    run_gcn_fixture("gcn_rmat4096_undirected.npz", src, dst, g["v_num"], True)
+
+
 def main():
+    parts = set(sys.argv[1:]) or {"walk", "plan", "gcn"}
+    if "gcn" in parts:
+        gcn_fixtures()
+    if "walk" not in parts and "plan" not in parts:
+        return
     # walks
     g1 = fb.synth_graph(seed=0, v_target=512, e_target=2048, holdout=0.1)
     run_walk_fixture("walk_rmat512.npz", g1["edges"], g1["v_num"], 20, 3, 7)

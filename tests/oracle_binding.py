@@ -104,8 +104,19 @@ def lib():
         L.orc_eval_choose.argtypes = [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, u32p]
         L.orc_walk_draw.argtypes = [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
                                     ctypes.c_uint32, ctypes.c_uint32, u32p, f64p]
+        L.orc_common_neighbours.argtypes = [u32p, u32p, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_int, i32p]
         _lib = L
     return _lib
+
+
+def common_neighbours(src, dst, v_num, undirected=True):
+    """orc_common_neighbours: per input edge, gcn.cpp's common-neighbour count."""
+    src = np.ascontiguousarray(src, np.uint32)
+    dst = np.ascontiguousarray(dst, np.uint32)
+    cn = np.zeros(len(src), np.int32)
+    rc = lib().orc_common_neighbours(ptr(src, u32p), ptr(dst, u32p), len(src), v_num, int(undirected), ptr(cn, i32p))
+    assert rc == 0, rc
+    return cn
 
 
 EDGE12 = np.dtype([("src", "<u4"), ("dst", "<u4"), ("data", "<f4")])
