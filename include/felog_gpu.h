@@ -340,7 +340,16 @@ felog_status felog_mlp_predict(felog_ctx *ctx, uint8_t *count, float *confidence
 
 /* ---- whole loop ---- */
 felog_status felog_run(felog_ctx *ctx, felog_run_stats *stats);
+/* -emb_output (word2vec.cu:2112-2127): "<V> <dim>\n", then per vocabulary row
+ * "<vertex> " + dim x "%lf " + "\n" (-binary 1: the dim floats raw).  Text rows
+ * are formatted by all host threads with felog_format_lf's formatter and
+ * written in order; the bytes equal the reference's serial fprintf. */
 felog_status felog_write_embeddings(felog_ctx *ctx, const char *path);
+/* The text writer's number formatter (no reference counterpart): each of the
+ * n floats as printf("%lf ") prints it (exact value rounded to six decimals,
+ * ties to even).  out: cap bytes; *len: bytes written.  FELOG_INVALID_ARG when
+ * cap is too small. */
+felog_status felog_format_lf(const float *x, uint64_t n, char *out, uint64_t cap, uint64_t *len);
 
 /* Kernels this library has launched on the context (diagnostics). */
 uint64_t felog_kernel_launches(const felog_ctx *ctx);

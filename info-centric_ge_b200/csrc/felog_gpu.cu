@@ -15,6 +15,7 @@
 #include <numeric>
 #include <random>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "budget.cuh"
@@ -2257,6 +2258,93 @@ extern "C" felog_status felog_run(felog_ctx *c, felog_run_stats *st) {
   return FELOG_OK;
 }
 
+namespace {
+// "%lf" of a float, as glibc prints it: the exact binary value rounded to six
+// decimals, ties to even.  A finite float is M * 2^E with M < 2^24; M * 10^6
+// fits in 64 bits, so shifting it by -E with round-half-even gives the six-
+// decimal integer exactly.  Values of 2^40 and above and non-finite values go
+// to snprintf.  Returns the number of characters written to out (>= 48 bytes).
+int format_lf(float x, char *out) {
+  uint32_t bits;
+  memcpy(&bits, &x, 4);
+  const int exp_field = (int)((bits >> 23) & 0xFF);
+  if (exp_field == 0xFF || (exp_field - 127) >= 40) return snprintf(out, 48, "%lf", (double)x);
+  const bool neg = bits >> 31;
+  uint64_t mant = bits & 0x7FFFFFu;
+  int e2;
+  if (exp_field == 0) {
+    e2 = -149;  // subnormal: M * 2^-149
+  } else {
+    mant |= 0x800000u;
+    e2 = exp_field - 150;
+  }
+  unsigned __int128 p = (unsigned __int128)mant * 1000000u;
+  uint64_t q;
+  if (e2 >= 0) {
+    q = (uint64_t)(p << e2);
+  } else {
+    const int sh = -e2;
+    if (sh >= 100) {
+      q = 0;  // p < 2^44 < half of 2^sh
+    } else {
+      const unsigned __int128 one = 1;
+      const unsigned __int128 rem = p & ((one << sh) - 1), half = one << (sh - 1);
+      q = (uint64_t)(p >> sh);
+      if (rem > half || (rem == half && (q & 1))) q++;
+    }
+  }
+  char tmp[32];
+  int n = 0;
+  const uint64_t ip = q / 1000000u;
+  uint32_t fr = (uint32_t)(q % 1000000u);
+  for (int i = 0; i < 6; i++) {
+    tmp[n++] = (char)('0' + fr % 10);
+    fr /= 10;
+  }
+  tmp[n++] = '.';
+  uint64_t v = ip;
+  do {
+    tmp[n++] = (char)('0' + v % 10);
+    v /= 10;
+  } while (v);
+  int k = 0;
+  if (neg) out[k++] = '-';
+  while (n) out[k++] = tmp[--n];
+  return k;
+}
+
+// Rows [a0, a1) of the word2vec text format: "<vertex> " + dim x "%lf " + "\n".
+void format_rows(const float *s0, const uint32_t *vertex, long long a0, long long a1, int dim, std::string &buf) {
+  buf.clear();
+  char tmp[64];
+  for (long long a = a0; a < a1; a++) {
+    int k = snprintf(tmp, sizeof tmp, "%u ", vertex[a]);
+    buf.append(tmp, (size_t)k);
+    for (int b = 0; b < dim; b++) {
+      k = format_lf(s0[(uint64_t)a * dim + b], tmp);
+      tmp[k++] = ' ';
+      buf.append(tmp, (size_t)k);
+    }
+    buf.push_back('\n');
+  }
+}
+}  // namespace
+
+extern "C" felog_status felog_format_lf(const float *x, uint64_t n, char *out, uint64_t cap, uint64_t *len) {
+  if ((n && !x) || (cap && !out)) return FELOG_INVALID_ARG;
+  uint64_t k = 0;
+  char tmp[64];
+  for (uint64_t i = 0; i < n; i++) {
+    const int m = format_lf(x[i], tmp);
+    if (k + (uint64_t)m + 1 > cap) return FELOG_INVALID_ARG;
+    memcpy(out + k, tmp, (size_t)m);
+    k += (uint64_t)m;
+    out[k++] = ' ';
+  }
+  if (len) *len = k;
+  return FELOG_OK;
+}
+
 extern "C" felog_status felog_write_embeddings(felog_ctx *c, const char *path) {
   if (!c || !path) return FELOG_INVALID_ARG;
   if (!c->model_ready) return fail(c, FELOG_NOT_READY, "model not initialised");
@@ -2267,16 +2355,30 @@ extern "C" felog_status felog_write_embeddings(felog_ctx *c, const char *path) {
   FILE *fo = fopen(path, "wb");
   if (!fo) return fail(c, FELOG_IO_ERROR, "cannot open %s", path);
   // word2vec.cu:2121-2127
-  fprintf(fo, "%lld %lld\n", (long long)c->vocab_size, (long long)dim);
-  for (long long a = 0; a < c->vocab_size; a++) {
-    fprintf(fo, "%u ", c->h_vocab_vertex[a]);
-    if (c->o.binary) {
-      fwrite(&s0[(uint64_t)a * dim], sizeof(float), dim, fo);
-    } else {
-      for (int b = 0; b < dim; b++) fprintf(fo, "%lf ", s0[(uint64_t)a * dim + b]);
+  bool ok = fprintf(fo, "%lld %lld\n", (long long)c->vocab_size, (long long)dim) > 0;
+  if (c->o.binary) {
+    for (long long a = 0; ok && a < c->vocab_size; a++) {
+      ok = fprintf(fo, "%u ", c->h_vocab_vertex[a]) > 0 &&
+           fwrite(&s0[(uint64_t)a * dim], sizeof(float), dim, fo) == (size_t)dim && fputc('\n', fo) != EOF;
     }
-    fprintf(fo, "\n");
+  } else {
+    // text: blocks of rows formatted by all host threads, written in order
+    const int nt = (int)std::max(1u, std::min(64u, std::thread::hardware_concurrency()));
+    const long long rows_per_block = 4096LL * nt;
+    std::vector<std::string> bufs((size_t)nt);
+    for (long long b0 = 0; ok && b0 < c->vocab_size; b0 += rows_per_block) {
+      const long long b1 = std::min<long long>(c->vocab_size, b0 + rows_per_block);
+      const long long per = (b1 - b0 + nt - 1) / nt;
+      std::vector<std::thread> th;
+      for (int t = 0; t < nt; t++) {
+        const long long r0 = std::min(b1, b0 + t * per), r1 = std::min(b1, r0 + per);
+        th.emplace_back(format_rows, s0.data(), c->h_vocab_vertex.data(), r0, r1, dim, std::ref(bufs[(size_t)t]));
+      }
+      for (auto &t : th) t.join();
+      for (int t = 0; ok && t < nt; t++)
+        ok = fwrite(bufs[(size_t)t].data(), 1, bufs[(size_t)t].size(), fo) == bufs[(size_t)t].size();
+    }
   }
-  if (fclose(fo) != 0) return fail(c, FELOG_IO_ERROR, "write failed on %s", path);
+  if (fclose(fo) != 0 || !ok) return fail(c, FELOG_IO_ERROR, "write failed on %s", path);
   return FELOG_OK;
 }

@@ -143,6 +143,7 @@ def gpu_lib():
         L.felog_set_corpus.argtypes = [_P, _P, _P, ctypes.c_uint64]
         L.felog_get_visit_freq.argtypes = [_P, _P]
         L.felog_walk_ceiling.argtypes = [_P, _P, _P]
+        L.felog_format_lf.argtypes = [_P, ctypes.c_uint64, _P, ctypes.c_uint64, _P]
         L.felog_common_neighbours.argtypes = [_P, _P, _P, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_int, _P, _P]
         L.felog_init_model.argtypes = [_P]
         L.felog_vocab_info.argtypes = [_P, _P, _P]
@@ -554,3 +555,15 @@ def auc(scores, labels):
     s = np.ascontiguousarray(scores, np.float32)
     lab = np.ascontiguousarray(labels, np.uint8)
     return tools_lib().felog_auc(_addr(s), _addr(lab), len(s))
+
+
+def format_lf(values):
+    """felog_format_lf: the floats as printf("%lf ") prints them (host only)."""
+    x = np.ascontiguousarray(values, np.float32)
+    cap = 64 * len(x) + 1
+    buf = ctypes.create_string_buffer(cap)
+    n = ctypes.c_uint64()
+    st = gpu_lib().felog_format_lf(_addr(x) if len(x) else None, len(x), buf, cap, ctypes.byref(n))
+    if st != 0:
+        raise FelogError(st, "felog_format_lf failed")
+    return buf.raw[: n.value].decode()

@@ -53,6 +53,10 @@ def test_run_loop_terminates_and_writes_reference_format(tmp_path):
     assert first[0] == str(vv[0]) and first[-1] == "" and len(first) == 130  # "%s " + 128 x "%lf " (:2123-2125)
     assert first[1] == "%lf" % s0[0]
     assert len(lines) == V + 1
+    # the whole file equals a serial printf rendering of every row
+    rows = s0.reshape(vs, 128)
+    want = f"{V} 128\n" + "".join(f"{vv[a]} " + "".join("%f " % float(x) for x in rows[a]) + "\n" for a in range(vs))
+    assert open(p).read() == want
 
 
 def test_stopped_vertices_spawn_no_walkers():
