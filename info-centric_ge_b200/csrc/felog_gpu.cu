@@ -149,6 +149,8 @@ struct felog_ctx {
   DevBuf<uint8_t> bud_stop_round;
   DevBuf<float> feat, mlp_params, mlp_m1, mlp_m2, mlp_partial, mlp_norm, mlp_grad, pred_conf, pred_len;
   DevBuf<double> mlp_loss;
+  DevBuf<float2> mlp_bc;       // Adam bias corrections per step
+  DevBuf<uint32_t> mlp_step;   // first step of the epoch being replayed
   DevBuf<uint32_t> mlp_idx;
   DevBuf<uint8_t> mlp_ycount, pred_count;
   DevBuf<float> mlp_ylen;
@@ -365,7 +367,7 @@ extern "C" void felog_destroy(felog_ctx *c) {
   c->exp_table.release(); c->syn0.release(); c->syn1.release(); c->syn0_bf.release(); c->syn1_bf.release(); c->jump.release();
   c->p_cand.release(); c->p_draws.release(); c->p_cons.release(); c->p_kept.release(); c->p_blk.release();
   c->p_state.release(); c->p_neg_state.release(); c->p_out_off.release(); c->p_batch_first.release();
-  c->p_sen.release(); c->table_coarse.release(); c->walk_claim.release(); c->pr_count.release(); c->pr_off.release(); c->pr_rec.release(); c->pr_cstate.release(); c->pr_jump.release(); c->pr_cfirst.release(); c->p_negs.release(); c->sim.release(); c->bud_walks.release(); c->bud_len_sum.release(); c->bud_first_len.release(); c->bud_stop_round.release(); c->feat.release(); c->mlp_params.release(); c->mlp_m1.release(); c->mlp_m2.release(); c->mlp_partial.release(); c->mlp_norm.release(); c->mlp_grad.release(); c->pred_conf.release(); c->pred_len.release(); c->mlp_loss.release(); c->mlp_idx.release(); c->mlp_ycount.release(); c->pred_count.release(); c->mlp_ylen.release(); c->cub_tmp.release(); c->out_tmp.release();
+  c->p_sen.release(); c->table_coarse.release(); c->walk_claim.release(); c->pr_count.release(); c->pr_off.release(); c->pr_rec.release(); c->pr_cstate.release(); c->pr_jump.release(); c->pr_cfirst.release(); c->p_negs.release(); c->sim.release(); c->bud_walks.release(); c->bud_len_sum.release(); c->bud_first_len.release(); c->bud_stop_round.release(); c->feat.release(); c->mlp_params.release(); c->mlp_m1.release(); c->mlp_m2.release(); c->mlp_partial.release(); c->mlp_norm.release(); c->mlp_grad.release(); c->pred_conf.release(); c->pred_len.release(); c->mlp_loss.release(); c->mlp_bc.release(); c->mlp_step.release(); c->mlp_idx.release(); c->mlp_ycount.release(); c->pred_count.release(); c->mlp_ylen.release(); c->cub_tmp.release(); c->out_tmp.release();
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
   if (c->tm0) cudaEventDestroy(c->tm0);
@@ -2020,14 +2022,29 @@ extern "C" felog_status felog_mlp_train(felog_ctx *c, const felog_mlp_opts *opts
   CK(c->mlp_idx.ensure(n), "mlp_train");
   CK(c->mlp_loss.ensure(n / kMlpBatch + 2), "mlp_train");
   std::vector<double> lp(n / kMlpBatch + 2);
-  uint64_t steps = 0;
   double loss_first = 0, loss_last = 0;
   const float b1 = 0.9f, b2 = 0.999f;
-  for (int ep = 0; ep < o.epochs; ep++) {
-    std::shuffle(idx.begin(), idx.end(), rng);
-    CK(cudaMemcpyAsync(c->mlp_idx.p, idx.data(), 4 * n, cudaMemcpyHostToDevice, c->stream), "mlp_train");
-    uint64_t nblk_total = 0;
-    for (uint64_t b0 = 0; b0 < n; b0 += o.batch) {
+  // One epoch (a gradient and an Adam launch per batch, the same batches every
+  // epoch) is captured once as a CUDA graph and replayed; the Adam bias
+  // corrections come from a per-step table and the epoch's first step from
+  // device memory, so the captured launches stay the same.
+  const uint64_t n_batches = (n + o.batch - 1) / o.batch;
+  const uint64_t steps = n_batches * (uint64_t)o.epochs;
+  std::vector<float2> bct(steps);
+  for (uint64_t s1 = 1; s1 <= steps; s1++)
+    bct[s1 - 1] = make_float2(1.0f - std::pow(b1, (float)s1), 1.0f - std::pow(b2, (float)s1));
+  CK(c->mlp_bc.ensure(std::max<uint64_t>(steps, 1)), "mlp_train");
+  CK(c->mlp_step.ensure(1), "mlp_train");
+  CK(cudaMemcpyAsync(c->mlp_bc.p, bct.data(), sizeof(float2) * steps, cudaMemcpyHostToDevice, c->stream), "mlp_train");
+  uint64_t nblk_total = 0;
+  for (uint64_t b0 = 0; b0 < n; b0 += o.batch) nblk_total += (std::min<uint64_t>(o.batch, n - b0) + kMlpBatch - 1) / kMlpBatch;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  auto capture_epoch = [&]() -> cudaError_t {
+    cudaError_t e = cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return e;
+    uint64_t blk = 0, j = 0;
+    for (uint64_t b0 = 0; b0 < n; b0 += o.batch, j++) {
       const uint64_t nb = std::min<uint64_t>(o.batch, n - b0);
       const int blocks = (int)((nb + kMlpBatch - 1) / kMlpBatch);
       MlpGradArgs ga{};
@@ -2038,26 +2055,45 @@ extern "C" felog_status felog_mlp_train(felog_ctx *c, const felog_mlp_opts *opts
       ga.idx = c->mlp_idx.p + b0;
       ga.n = nb;
       ga.partial = c->mlp_partial.p;
-      ga.loss_partial = c->mlp_loss.p + nblk_total;
+      ga.loss_partial = c->mlp_loss.p + blk;
       k_mlp_grad<<<blocks, kMlpBatch, kMlpSmem, c->stream>>>(ga);
-      c->launches++;
-      steps++;
-      const float bc1 = 1.0f - std::pow(b1, (float)steps), bc2 = 1.0f - std::pow(b2, (float)steps);
       k_mlp_adam<<<(kMlpParams + 255) / 256, 256, 0, c->stream>>>(c->mlp_params.p, c->mlp_m1.p, c->mlp_m2.p,
                                                                   c->mlp_partial.p, blocks, 1.0f / (float)nb, o.lr,
-                                                                  b1, b2, 1e-8f, bc1, bc2, nullptr);
-      c->launches++;
-      nblk_total += blocks;
+                                                                  b1, b2, 1e-8f, 1.0f, 1.0f, nullptr, c->mlp_bc.p,
+                                                                  c->mlp_step.p, (uint32_t)j);
+      blk += blocks;
     }
-    CK(cudaGetLastError(), "mlp_train");
-    CK(cudaMemcpyAsync(lp.data(), c->mlp_loss.p, 8 * nblk_total, cudaMemcpyDeviceToHost, c->stream), "mlp_train");
-    CK(cudaStreamSynchronize(c->stream), "mlp_train");
+    const cudaError_t le = cudaGetLastError();
+    e = cudaStreamEndCapture(c->stream, &graph);
+    if (le != cudaSuccess) return le;
+    if (e != cudaSuccess) return e;
+    return cudaGraphInstantiate(&exec, graph, 0);
+  };
+  felog_status st = FELOG_OK;
+  std::vector<uint32_t> base(1);
+  for (int ep = 0; ep < o.epochs && st == FELOG_OK; ep++) {
+    std::shuffle(idx.begin(), idx.end(), rng);
+    cudaError_t e = cudaMemcpyAsync(c->mlp_idx.p, idx.data(), 4 * n, cudaMemcpyHostToDevice, c->stream);
+    base[0] = (uint32_t)(n_batches * (uint64_t)ep);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(c->mlp_step.p, base.data(), 4, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess && !exec) e = capture_epoch();
+    if (e == cudaSuccess) e = cudaGraphLaunch(exec, c->stream);
+    c->launches += 2 * n_batches;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(lp.data(), c->mlp_loss.p, 8 * nblk_total, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) {
+      st = cuda_fail(c, e, "mlp_train");
+      break;
+    }
     double l = 0;
     for (uint64_t i = 0; i < nblk_total; i++) l += lp[i];
     l /= (double)n;
     if (ep == 0) loss_first = l;
     loss_last = l;
   }
+  if (exec) cudaGraphExecDestroy(exec);
+  if (graph) cudaGraphDestroy(graph);
+  if (st != FELOG_OK) return st;
   c->mlp_ready = true;
   // fit on the training vertices
   CK(c->pred_count.ensure(V), "mlp_train");

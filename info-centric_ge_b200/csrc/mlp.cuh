@@ -231,8 +231,17 @@ __global__ void __launch_bounds__(kMlpBatch) k_mlp_grad(MlpGradArgs a) {
 }
 
 // sum the block partials in block order, divide by the batch size, Adam step
+// Bias corrections: bc1 / bc2, or, with bc_tab, entry *step_base + j of the
+// per-step table (a captured epoch replays with the step offset in device
+// memory).
 __global__ void k_mlp_adam(float *params, float *m1, float *m2, const float *partial, int blocks, float inv_n,
-                           float lr, float beta1, float beta2, float eps, float bc1, float bc2, float *grad_out) {
+                           float lr, float beta1, float beta2, float eps, float bc1, float bc2, float *grad_out,
+                           const float2 *bc_tab = nullptr, const uint32_t *step_base = nullptr, uint32_t j = 0) {
+  if (bc_tab) {
+    const float2 bc = bc_tab[*step_base + j];
+    bc1 = bc.x;
+    bc2 = bc.y;
+  }
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < kMlpParams; i += gridDim.x * blockDim.x) {
     float g = 0.0f;
     for (int b = 0; b < blocks; b++) g += partial[(uint64_t)b * kMlpParams + i];
