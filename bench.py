@@ -379,7 +379,15 @@ def bench_mine(args):
         sg_bytes = 2 * row_bytes * (cnt["pairs"] + (TRAIN["negative"] + 1) * cnt["kept"])
         sg_kernel = "k_sgns_reuse_tile_tc<128, 5>"
     else:
-        sg_bytes = cnt["pairs"] * SGNS_BYTES_PER_PAIR[prec]
+        # per pair: each referenced row (context + trained targets) read and
+        # written once; in the BF16 form the top-1% rows are FP32 master rows,
+        # counted at their FP32 size (shares from the last trained chunk)
+        mix_pairs, mix_refs, mix_hot = f.pair_row_mix()
+        refs_per_pair = mix_refs / mix_pairs
+        hot_share = mix_hot / mix_refs
+        per_ref = 2 * (512 * hot_share + 256 * (1 - hot_share)) if prec == "bf16" else 2 * 512
+        sg_bytes_per_pair = refs_per_pair * per_ref
+        sg_bytes = cnt["pairs"] * sg_bytes_per_pair
         sg_kernel = f"k_sgns_train_pairs<128, 5, Rows{prec.upper()}>"
     sg_achieved = sg_bytes / (cnt["train_ms"] * 1e-3) / 1e9
     walk_achieved = cnt["tokens"] * WALK_BYTES_PER_STEP / (cnt["walk_ms"] * 1e-3) / 1e9
@@ -413,6 +421,9 @@ def bench_mine(args):
                                  if FORMS[form]["reuse_neg"] == 0 else None),
                      "traffic_unit": "bytes per launch (ncu per-pair DRAM traffic x pairs per launch)", "achieved": sg_achieved, "peak": peak,
                      "unit": "GB/s", "frac": sg_achieved / peak,
+                     "algorithmic_bytes_per_pair": sg_bytes / max(cnt["pairs"], 1),
+                     "row_refs_per_pair": refs_per_pair if FORMS[form]["reuse_neg"] in (0, 1) else None,
+                     "master_row_share": hot_share if FORMS[form]["reuse_neg"] in (0, 1) else None,
                      "peak_source": peak_kind,
                      "walk_kernel": {"achieved": walk_achieved, "frac": walk_achieved / peak,
                                      "bytes_per_step": WALK_BYTES_PER_STEP,

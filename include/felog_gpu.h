@@ -252,6 +252,12 @@ felog_status felog_vocab_info(felog_ctx *ctx, uint64_t *vocab_size, uint64_t *tr
 felog_status felog_get_vocab(felog_ctx *ctx, uint32_t *vocab_vertex, uint32_t *id2offset);
 /* alpha < 0: take the schedule value of round `round` */
 felog_status felog_train_round(felog_ctx *ctx, uint32_t round, float alpha, felog_train_stats *stats);
+/* Row references of the last trained pair-stream chunk (no reference
+ * counterpart; for roofline accounting): pairs in the chunk, row references
+ * (each pair's context row and its trained target rows) and how many of them
+ * hit FP32 master rows (all of them in the FP32 form).  FELOG_NOT_READY before
+ * a skip-gram round over the pair stream. */
+felog_status felog_pair_row_mix(felog_ctx *ctx, uint64_t *pairs, uint64_t *row_refs, uint64_t *hot_refs);
 /* rows in vocabulary order, logical dimension order, FP32 */
 felog_status felog_get_embeddings(felog_ctx *ctx, float *syn0, float *syn1, uint64_t cap_floats);
 felog_status felog_set_embeddings(felog_ctx *ctx, const float *syn0, const float *syn1);

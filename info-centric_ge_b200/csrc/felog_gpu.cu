@@ -97,6 +97,8 @@ struct felog_ctx {
   DevBuf<uint32_t> sent_len;
   uint64_t n_sent = 0, n_tok = 0;
   uint64_t last_walk_tokens = 0, last_walk_traces = 0;  // totals of the last walk round
+  uint64_t last_chunk_pairs = 0;  // pair records of the last trained chunk (still in pr_rec)
+  int last_chunk_stride = 0;
   bool corpus_ready = false;
   DevBuf<unsigned int> visit_freq;
   uint64_t words_sum_cum = 0;
@@ -910,6 +912,25 @@ extern "C" felog_status felog_common_neighbours(felog_ctx *c, const uint32_t *sr
   return s;
 }
 
+extern "C" felog_status felog_pair_row_mix(felog_ctx *c, uint64_t *pairs, uint64_t *row_refs, uint64_t *hot_refs) {
+  if (!c || !pairs || !row_refs || !hot_refs) return FELOG_INVALID_ARG;
+  if (!c->last_chunk_pairs) return fail(c, FELOG_NOT_READY, "pair_row_mix: no pair-stream chunk trained yet");
+  CK(cudaSetDevice(c->device), "pair_row_mix");
+  CK(cudaMemsetAsync(c->counters.p + 12, 0, 16, c->stream), "pair_row_mix");
+  const uint64_t n = c->last_chunk_pairs;
+  k_pair_row_mix<<<grid_for(c, n, 256), 256, 0, c->stream>>>(c->pr_rec.p, n, c->last_chunk_stride,
+                                                             c->o.negative + 1, (uint32_t)c->n_f32,
+                                                             c->counters.p + 12);
+  c->launches++;
+  CK(cudaGetLastError(), "pair_row_mix");
+  unsigned long long h[2];
+  RB(h, c->counters.p + 12, sizeof h, "pair_row_mix");
+  *pairs = n;
+  *row_refs = h[0];
+  *hot_refs = h[1];
+  return FELOG_OK;
+}
+
 extern "C" felog_status felog_corpus_size(felog_ctx *c, uint64_t *n_sentences, uint64_t *n_tokens) {
   if (!c) return FELOG_INVALID_ARG;
   if (!c->corpus_ready) return fail(c, FELOG_NOT_READY, "no corpus");
@@ -1364,6 +1385,8 @@ felog_status train_pairs(felog_ctx *c, SgArgs g, int blocks, int threads) {
     pa.s0 = ch.first;
     pa.s1 = ch.second;
     pa.base = total > kPairChunk ? c->h_pr_off[ch.first] : 0;
+    c->last_chunk_pairs = total > kPairChunk ? c->h_pr_off[ch.second] - c->h_pr_off[ch.first] : total;
+    c->last_chunk_stride = stride;
     const int eb = grid_for(c, (ch.second - ch.first) * 32, 256);
     if (K == 5) k_pair_emit<5><<<eb, 256, 0, c->stream>>>(pa);
     else k_pair_emit<7><<<eb, 256, 0, c->stream>>>(pa);

@@ -791,4 +791,31 @@ __global__ void __launch_bounds__(32 * kTileWarps) k_sgns_reuse_tile_tc(SgArgs a
   if (lane == 0 && my_pairs) atomicAdd(a.pairs, my_pairs);
 }
 
+// Row references of a chunk of pair records: per pair its context row and
+// every target row that is trained (a skipped negative is -1), and how many of
+// them are FP32 master rows (row < n_hot).  out[0] += references, out[1] +=
+// master-row references.
+__global__ void k_pair_row_mix(const int32_t *__restrict__ rec, uint64_t n, int stride, int nt, uint32_t n_hot,
+                               unsigned long long *out) {
+  unsigned long long refs = 0, hot = 0;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const int32_t *r = rec + i * (uint64_t)stride;
+    refs++;
+    hot += (uint32_t)r[0] < n_hot;
+    for (int q = 0; q < nt; q++) {
+      const int32_t t = r[1 + q];
+      refs += t >= 0;
+      hot += t >= 0 && (uint32_t)t < n_hot;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    refs += __shfl_down_sync(0xffffffffu, refs, o);
+    hot += __shfl_down_sync(0xffffffffu, hot, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (refs) atomicAdd(&out[0], refs);
+    if (hot) atomicAdd(&out[1], hot);
+  }
+}
+
 }  // namespace felog

@@ -143,6 +143,7 @@ def gpu_lib():
         L.felog_set_corpus.argtypes = [_P, _P, _P, ctypes.c_uint64]
         L.felog_get_visit_freq.argtypes = [_P, _P]
         L.felog_walk_ceiling.argtypes = [_P, _P, _P]
+        L.felog_pair_row_mix.argtypes = [_P, _P, _P, _P]
         L.felog_format_lf.argtypes = [_P, ctypes.c_uint64, _P, ctypes.c_uint64, _P]
         L.felog_common_neighbours.argtypes = [_P, _P, _P, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_int, _P, _P]
         L.felog_init_model.argtypes = [_P]
@@ -320,6 +321,13 @@ class Felog:
         self._ck(self._L.felog_common_neighbours(self.h, _addr(src), _addr(dst), len(src), v_num, int(undirected),
                                                  _addr(cn), ctypes.byref(ms)))
         return cn, ms.value
+
+    def pair_row_mix(self):
+        """felog_pair_row_mix: (pairs, row references, master-row references)
+        of the last trained pair-stream chunk."""
+        v = [ctypes.c_uint64() for _ in range(3)]
+        self._ck(self._L.felog_pair_row_mix(self.h, *[ctypes.byref(x) for x in v]))
+        return tuple(x.value for x in v)
 
     def walk_ceiling(self):
         """Memory skeleton of the last walk round (felog_walk_ceiling):

@@ -249,3 +249,26 @@ def test_cbow_deterministic_matches_oracle(dim, negative):
     np.testing.assert_allclose(g1, r1, rtol=RTOL, atol=1e-7)
     exact = np.mean(g0 == r0), np.mean(g1 == r1)
     print("cbow fraction bit-exact syn0/syn1:", exact)
+
+
+def test_pair_row_mix_counts_master_rows():
+    """felog_pair_row_mix: row references of the last pair-stream chunk; every
+    reference is a master row in the FP32 form, a share of them in BF16."""
+    g = fb.synth_graph(seed=6, v_target=8192, e_target=65536, holdout=0.0)
+    V = g["v_num"]
+    out = {}
+    for prec in (0, 1):
+        f = fb.Felog(v_num=V, size=128, window=10, negative=5, sample=1e-3, cbow=0, reuse_neg=0, min_count=0,
+                     seed=3, precision=prec)
+        f.load_graph(g["edges"], V)
+        f.init_model()
+        with pytest.raises(fb.FelogError):
+            f.pair_row_mix()
+        f.walk_round(0)
+        ts = f.train_round(0)
+        out[prec] = f.pair_row_mix()
+        f.close()
+        pairs, refs, hot = out[prec]
+        assert pairs == ts["pairs"] and pairs < refs <= 7 * pairs
+    assert out[0][2] == out[0][1]
+    assert 0 < out[1][2] < out[1][1]
