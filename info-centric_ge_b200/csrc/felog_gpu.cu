@@ -539,7 +539,11 @@ extern "C" felog_status felog_get_alias(felog_ctx *c, float *prob, uint32_t *ali
 extern "C" felog_status felog_set_stop_flags(felog_ctx *c, const uint8_t *flags) {
   if (!c || !flags) return FELOG_INVALID_ARG;
   if (!c->V) return fail(c, FELOG_NOT_READY, "no graph loaded");
-  CK(cudaMemcpy(c->stop.p, flags, c->V, cudaMemcpyHostToDevice), "set_stop_flags");
+  CK(cudaSetDevice(c->device), "set_stop_flags");
+  // work still queued on the context's stream (a snapshot for an asynchronous
+  // copy) finishes before the flags change
+  CK(cudaMemcpyAsync(c->stop.p, flags, c->V, cudaMemcpyHostToDevice, c->stream), "set_stop_flags");
+  CK(cudaStreamSynchronize(c->stream), "set_stop_flags");
   return FELOG_OK;
 }
 
@@ -1478,6 +1482,7 @@ extern "C" felog_status felog_train_round(felog_ctx *c, uint32_t round, float al
   float ms_plan = 0, ms_train = 0;
   CK(cudaMemsetAsync(c->counters.p, 0, sizeof(unsigned long long) * 16, c->stream), "train_round");
   CK(cudaMemsetAsync(c->derr.p, 0, sizeof(int), c->stream), "train_round");
+  c->last_chunk_pairs = 0;  // set again if this round trains over the pair stream
   felog_status s = plan_round(c, &ms_plan);
   if (s != FELOG_OK) return s;
   CK(cudaMemsetAsync(c->counters.p, 0, sizeof(unsigned long long) * 4, c->stream), "train_round");
@@ -1706,6 +1711,9 @@ extern "C" felog_status felog_set_embeddings(felog_ctx *c, const float *syn0, co
   if (!c->model_ready) return fail(c, FELOG_NOT_READY, "model not initialised");
   const int dim = c->o.size;
   const uint64_t nf = (uint64_t)c->n_f32 * dim, nel = (uint64_t)c->vocab_size * dim;
+  CK(cudaSetDevice(c->device), "set_embeddings");
+  // a snapshot still queued for an asynchronous copy reads the rows first
+  CK(cudaStreamSynchronize(c->stream), "set_embeddings");
   std::vector<float> buf(nf);
   std::vector<uint16_t> bbuf(nel - nf);
   for (int which = 0; which < 2; which++) {
