@@ -1289,6 +1289,9 @@ void launch_pairs_dkp(felog_ctx *c, const SgArgs &g, int blocks, int threads, ui
   else if (minb == 3)
     k_sgns_train_pairs<D, K, P, (D >= 256 ? 2 : 3)><<<blocks, threads, 0, c->stream>>>(g, c->pr_rec.p, c->pr_off.p, base,
                                                                                       s0);
+  else if (minb == 5)
+    k_sgns_train_pairs<D, K, P, (D >= 256 ? 2 : 5)><<<blocks, threads, 0, c->stream>>>(g, c->pr_rec.p, c->pr_off.p, base,
+                                                                                      s0);
   else
     k_sgns_train_pairs<D, K, P, (D >= 256 ? 2 : 4)><<<blocks, threads, 0, c->stream>>>(g, c->pr_rec.p, c->pr_off.p, base,
                                                                                       s0);
@@ -1396,17 +1399,19 @@ felog_status train_pairs(felog_ctx *c, SgArgs g, int blocks, int threads) {
     else k_pair_emit<7><<<eb, 256, 0, c->stream>>>(pa);
     c->launches++;
     // launch-shape autotuner: the first chunk of the first tuned round is
-    // trained in three slices of sentences, one per candidate register budget
-    // (real work, nothing repeated); the fastest per pair is kept
+    // trained in four slices of sentences, one per candidate register budget
+    // (5, 4, 3 or 2 resident blocks per SM; real work, nothing repeated); the
+    // fastest per pair is kept
     const uint64_t nch = ch.second - ch.first;
+    constexpr int kCand = 4;
     if (c->o.autotune && !c->o.deterministic && c->o.size <= 128 && c->pair_minb == 0 &&
-        nch >= 3 * (uint64_t)blocks * (threads / 32)) {
-      const int cand[3] = {4, 3, 2};
-      cudaEvent_t ev[4];
-      for (int i = 0; i < 4; i++) CK(cudaEventCreate(&ev[i]), "autotune");
-      uint64_t bound[4];
-      for (int i = 0; i <= 3; i++) bound[i] = ch.first + nch * i / 3;
-      for (int i = 0; i < 3; i++) {
+        nch >= kCand * (uint64_t)blocks * (threads / 32)) {
+      const int cand[kCand] = {5, 4, 3, 2};
+      cudaEvent_t ev[kCand + 1];
+      for (int i = 0; i <= kCand; i++) CK(cudaEventCreate(&ev[i]), "autotune");
+      uint64_t bound[kCand + 1];
+      for (int i = 0; i <= kCand; i++) bound[i] = ch.first + nch * i / kCand;
+      for (int i = 0; i < kCand; i++) {
         CK(cudaMemsetAsync(c->counters.p + 0, 0, 8, c->stream), "train");
         SgArgs gi = g;
         gi.n_sent = bound[i + 1] - bound[i];
@@ -1422,14 +1427,14 @@ felog_status train_pairs(felog_ctx *c, SgArgs g, int blocks, int threads) {
         c->launches++;
         CK(cudaGetLastError(), "train_round: launch");
       }
-      CK(cudaEventRecord(ev[3], c->stream), "autotune");
-      uint64_t offs[4];
-      for (int i = 0; i <= 3; i++) RB(&offs[i], c->pr_off.p + bound[i], 8, "autotune");
+      CK(cudaEventRecord(ev[kCand], c->stream), "autotune");
+      uint64_t offs[kCand + 1];
+      for (int i = 0; i <= kCand; i++) RB(&offs[i], c->pr_off.p + bound[i], 8, "autotune");
       double best = 1e300;
       int pick = 4;
       char buf[256];
       std::string rep = "pair trainer blocks/SM:";
-      for (int i = 0; i < 3; i++) {
+      for (int i = 0; i < kCand; i++) {
         float ms = 0;
         CK(cudaEventElapsedTime(&ms, ev[i], ev[i + 1]), "autotune");
         const double per = ms / (double)std::max<uint64_t>(1, offs[i + 1] - offs[i]);
@@ -1443,7 +1448,7 @@ felog_status train_pairs(felog_ctx *c, SgArgs g, int blocks, int threads) {
       snprintf(buf, sizeof buf, "; chose %d", pick);
       c->tuning = rep + buf;
       c->pair_minb = pick;
-      for (int i = 0; i < 4; i++) cudaEventDestroy(ev[i]);
+      for (int i = 0; i <= kCand; i++) cudaEventDestroy(ev[i]);
       continue;
     }
     CK(cudaMemsetAsync(c->counters.p + 0, 0, 8, c->stream), "train");  // sentence claim counter

@@ -386,7 +386,7 @@ __device__ __forceinline__ int rec_at(const int4 (&v)[S / 4], int i) {
 // negatives repeat a row takes the sequential path, where the later target
 // sees the earlier update as in the reference.
 // MINB: resident 256-thread blocks per SM the register budget is built for
-// (the launch-shape autotuner picks among 2, 3 and 4 for DIM <= 128).
+// (the launch-shape autotuner picks among 2, 3, 4 and 5 for DIM <= 128).
 template <int DIM, int NK, class P, int MINB = (DIM >= 256 ? 2 : 4)>
 __global__ void __launch_bounds__(256, MINB)
     k_sgns_train_pairs(SgArgs a, const int32_t *__restrict__ rec, const uint64_t *__restrict__ off, uint64_t base,
