@@ -1284,7 +1284,8 @@ void launch_trainer(felog_ctx *c, const SgArgs &g, int blocks, int threads) {
 
 template <int D, int K, class P>
 void launch_pairs_dkp(felog_ctx *c, const SgArgs &g, int blocks, int threads, uint64_t base, uint64_t s0) {
-  const int minb = D >= 256 ? 2 : (c->pair_minb ? c->pair_minb : 4);
+  // untuned: 5 blocks per SM for BF16 rows (48 registers), 4 for FP32 rows (5 spills)
+  const int minb = D >= 256 ? 2 : (c->pair_minb ? c->pair_minb : (P::kBF16 ? 5 : 4));
   if (minb == 2) k_sgns_train_pairs<D, K, P, 2><<<blocks, threads, 0, c->stream>>>(g, c->pr_rec.p, c->pr_off.p, base, s0);
   else if (minb == 3)
     k_sgns_train_pairs<D, K, P, (D >= 256 ? 2 : 3)><<<blocks, threads, 0, c->stream>>>(g, c->pr_rec.p, c->pr_off.p, base,
