@@ -177,7 +177,9 @@ int felog_abi_version(void);
 
 /* ---- graph ---- */
 /* n records of the 12-byte binary format; doubled (e, e^T interleaved) when
- * undirected; CSR bucketed by source in record order (graph.hpp:531-575). */
+ * undirected; CSR bucketed by source in record order (graph.hpp:531-575).
+ * Limits: at most 2^31-1 CSR entries and 2^31-2 vertices (FELOG_INVALID_ARG
+ * beyond; the build sorts and scans with 32-bit counts). */
 felog_status felog_load_graph(felog_ctx *ctx, const felog_edge12 *edges, uint64_t n, uint32_t v_num,
                               int undirected);
 felog_status felog_load_graph_file(felog_ctx *ctx, const char *path, uint32_t v_num, int undirected);

@@ -388,7 +388,9 @@ extern "C" felog_status felog_load_graph(felog_ctx *c, const felog_edge12 *edges
   if (v_num == 0) return fail(c, FELOG_INVALID_ARG, "load_graph: v_num must be > 0");
   if (n && !edges) return fail(c, FELOG_INVALID_ARG, "load_graph: edges is NULL");
   uint64_t m = undirected ? 2 * n : n;
-  if (m >= 0xFFFFFFFFULL) return fail(c, FELOG_INVALID_ARG, "load_graph: more than 2^32-1 CSR entries");
+  // the CSR build sorts and scans with 32-bit signed counts
+  if (m > 0x7FFFFFFFULL) return fail(c, FELOG_INVALID_ARG, "load_graph: more than 2^31-1 CSR entries");
+  if (v_num > 0x7FFFFFFEu) return fail(c, FELOG_INVALID_ARG, "load_graph: more than 2^31-2 vertices");
   // the previous graph is gone as soon as its buffers are reused
   c->V = 0;
   c->M = 0;
@@ -639,6 +641,7 @@ extern "C" felog_status felog_walk_round(felog_ctx *c, uint32_t round, const fel
   if (c->o.weighted && !c->has_alias) return fail(c, FELOG_NOT_READY, "weighted walk needs felog_build_alias");
   CK(cudaSetDevice(c->device), "walk_round");
   const uint32_t walker_num = c->o.walker_num ? c->o.walker_num : c->V;
+  if (walker_num > 0x7FFFFFFEu) return fail(c, FELOG_INVALID_ARG, "walk_round: more than 2^31-2 walkers");
   felog_status s = build_active(c, walker_num);
   if (s != FELOG_OK) return s;
   const uint32_t na = c->n_active;
