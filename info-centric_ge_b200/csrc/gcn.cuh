@@ -128,9 +128,16 @@ __global__ void k_gcn_edges(const uint32_t *__restrict__ src, const uint32_t *__
   }
 }
 
-// Warp per listed edge: lanes take short elements j = lane, lane + 32, ...; a
-// match that equals the previous short element or s or d is one decrement,
-// except at the first match, where only s or d counts (and then separately).
+// Warp per listed edge; a match that equals the previous short element or s
+// or d is one decrement, except at the first match, where only s or d counts
+// (and then separately).  Lists of comparable length (long <= kGcnMergeRatio x
+// short) are merged: each lane takes an equal share of the merge steps (its
+// start found by a diagonal binary search), and the merge takes the short
+// element first on ties, so a short element is matched exactly when the long
+// element in front of it is equal, and a repeated short element matches
+// again.  Otherwise lanes take short elements j = lane, lane + 32, ... with a
+// binary search of the long list each.
+constexpr uint64_t kGcnMergeRatio = 4;
 __global__ void k_gcn_heavy(const uint32_t *__restrict__ src, const uint32_t *__restrict__ dst,
                             const uint32_t *__restrict__ heavy, const unsigned long long *__restrict__ n_heavy,
                             const uint64_t *__restrict__ row_ptr, const uint32_t *__restrict__ nbr,
@@ -144,14 +151,43 @@ __global__ void k_gcn_heavy(const uint32_t *__restrict__ src, const uint32_t *__
     const GcnLists g = gcn_lists(row_ptr, s, d);
     uint32_t total = 0, flagged = 0;
     uint64_t j0 = ~0ULL;
-    for (uint64_t j = lane; j < g.sn; j += 32) {
-      const uint32_t x = nbr[g.sb + j];
-      const uint64_t p = gcn_lower(nbr, g.lb, g.lb + g.ln, x);
-      if (p < g.lb + g.ln && nbr[p] == x) {
-        total++;
-        if (j < j0) j0 = j;
-        const bool dup = j > 0 && nbr[g.sb + j - 1] == x;
-        flagged += (dup || x == s || x == d) ? 1u : 0u;
+    if (g.ln <= kGcnMergeRatio * g.sn) {
+      const uint32_t *S = nbr + g.sb, *L = nbr + g.lb;
+      const uint64_t ns = g.sn, nl = g.ln, seg = (ns + nl + 31) / 32;
+      const uint64_t dg = lane * seg < ns + nl ? lane * seg : ns + nl;
+      // i = short elements among the first dg merged ones
+      uint64_t lo = dg > nl ? dg - nl : 0, hi = dg < ns ? dg : ns;
+      while (lo < hi) {
+        const uint64_t mid = (lo + hi) >> 1;
+        if (S[mid] <= L[dg - mid - 1]) lo = mid + 1;
+        else hi = mid;
+      }
+      uint64_t i = lo, j = dg - lo;
+      uint32_t prev = i > 0 ? S[i - 1] : 0;
+      for (uint64_t step = 0; step < seg && (i < ns || j < nl); step++) {
+        if (i < ns && (j >= nl || S[i] <= L[j])) {
+          const uint32_t x = S[i];
+          if (j < nl && L[j] == x) {
+            total++;
+            if (i < j0) j0 = i;
+            flagged += ((i > 0 && prev == x) || x == s || x == d) ? 1u : 0u;
+          }
+          prev = x;
+          i++;
+        } else {
+          j++;
+        }
+      }
+    } else {
+      for (uint64_t j = lane; j < g.sn; j += 32) {
+        const uint32_t x = nbr[g.sb + j];
+        const uint64_t p = gcn_lower(nbr, g.lb, g.lb + g.ln, x);
+        if (p < g.lb + g.ln && nbr[p] == x) {
+          total++;
+          if (j < j0) j0 = j;
+          const bool dup = j > 0 && nbr[g.sb + j - 1] == x;
+          flagged += (dup || x == s || x == d) ? 1u : 0u;
+        }
       }
     }
     for (int o = 16; o > 0; o >>= 1) {
