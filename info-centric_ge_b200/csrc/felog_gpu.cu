@@ -39,6 +39,10 @@ template <class T>
 struct DevBuf {
   T *p = nullptr;
   size_t n = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf &) = delete;
+  DevBuf &operator=(const DevBuf &) = delete;
+  ~DevBuf() { release(); }  // temporaries are freed on every return path
   cudaError_t ensure(size_t want) {
     if (want <= n && p) return cudaSuccess;
     if (p) cudaFree(p);
