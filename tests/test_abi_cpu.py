@@ -35,6 +35,10 @@ def test_default_opts_follow_reference_defaults():
     assert (o.size, o.window, o.negative, o.cbow, o.reuse_neg, o.hs, o.iter, o.min_count) == (100, 5, 5, 1, 1, 0, 5, 5)
     assert abs(o.sample - 1e-3) < 1e-9 and abs(o.alpha - 0.025) < 1e-9
     assert (o.min_length, o.min_rounds, o.eval_batch_size) == (20, 5, 16384)
+    # the Python mirror of felog_opts matches the C layout to its last field
+    assert ctypes.sizeof(fb.FelogOpts) == 160
+    assert (o.seed, o.slot_len, o.hot_rows, o.autotune) == (0x5EED0001, 64, 0, 1)
+    assert o.budget_confidence == 0.0 and o.budget_audit == 0.0
 
 
 def test_create_reports_status_without_crashing():
