@@ -493,7 +493,7 @@ __global__ void __launch_bounds__(256, MINB)
 // reads and writes n + K + 1 rows instead of 2 (K + 1) n for the pair-by-pair
 // order, n being the number of contexts.
 template <int DIM, int NK, class P>
-__global__ void __launch_bounds__(256, 3) k_sgns_reuse_tile(SgArgs a) {
+__global__ void __launch_bounds__(256, 4) k_sgns_reuse_tile(SgArgs a) {
   static_assert(DIM >= 64, "two or more values per lane");
   constexpr int H = DIM / 64;
   constexpr int NT = NK + 1;
