@@ -24,3 +24,50 @@ def test_oracle_small_cases_by_hand():
     src2 = np.concatenate([src, [0]]).astype(np.uint32)
     dst2 = np.concatenate([dst, [1]]).astype(np.uint32)
     np.testing.assert_array_equal(ob.common_neighbours(src2, dst2, 4), [1, 1, 1, 0, 1])
+
+
+def definition(src, dst, V, undirected):
+    """The count as the GPU kernels state it: for an edge (s, d), the elements
+    of the shorter sorted neighbour list (N(s) on a tie) that occur in the
+    longer one, in order; minus one for a leading s or d; while more than one
+    is left, minus one for every later element equal to its predecessor or to
+    s or d.  Every edge of an unordered pair reports its first edge's count."""
+    rows = [[] for _ in range(V)]
+    for s, d in zip(src, dst):
+        rows[s].append(d)
+        if undirected:
+            rows[d].append(s)
+    rows = [sorted(r) for r in rows]
+    first, out = {}, []
+    for e, (s, d) in enumerate(zip(src, dst)):
+        key = (min(s, d), max(s, d))
+        if key not in first:
+            a, b = rows[s], rows[d]
+            short, long_ = (b, a) if len(a) > len(b) else (a, b)
+            longset = set(long_)
+            inter = [x for x in short if x in longset]
+            c = len(inter)
+            if c > 0:
+                if inter[0] in (s, d):
+                    c -= 1
+                if c > 1:
+                    for i in range(1, len(inter)):
+                        if inter[i] == inter[i - 1] or inter[i] in (s, d):
+                            c -= 1
+            first[key] = c
+        out.append(first[key])
+    return np.array(out, np.int32)
+
+
+@pytest.mark.parametrize("seed,undirected", [(1, True), (2, False), (3, True), (4, False)])
+def test_oracle_galloping_equals_definition(seed, undirected):
+    rng = np.random.default_rng(seed)
+    V = 40
+    n = 400
+    src = rng.integers(0, V, n).astype(np.uint32)
+    dst = (src + rng.zipf(1.5, n) % V).astype(np.uint32) % V
+    if not undirected:  # every vertex keeps an out-edge
+        src = np.concatenate([src, np.arange(V, dtype=np.uint32)])
+        dst = np.concatenate([dst, (np.arange(V, dtype=np.uint32) + 1) % V])
+    got = ob.common_neighbours(src, dst, V, undirected)
+    np.testing.assert_array_equal(got, definition(src.tolist(), dst.tolist(), V, undirected))
