@@ -464,11 +464,17 @@ def bench_reference(args):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_pipeline was not built"}))
         return
     cfg = CONFIGS[args.config]
-    g = make_graph(cfg)
     import tempfile
     with tempfile.TemporaryDirectory() as td:
         gp = os.path.join(td, "g.bin")
-        g["edges"].tofile(gp)
+        # the graph comes from a child process, so this process maps none of
+        # the repository's libraries
+        gen = subprocess.run([sys.executable, os.path.abspath(__file__), "--config", args.config,
+                              "--write-graph", gp], capture_output=True, text=True)
+        if gen.returncode != 0:
+            print(json.dumps({"impl": "reference", "unavailable": f"graph generation failed: {gen.stderr[-200:]}"}))
+            return
+        g = json.loads(gen.stdout.strip().splitlines()[-1])
         cmd = [exe, gp, str(g["v_num"]), str(args.warmup), str(args.steps), str(args.ref_walkers)]
         log("reference:", " ".join(cmd))
         res = subprocess.run(cmd, capture_output=True, text=True)
@@ -564,7 +570,15 @@ def main():
                     help="keep the default launch shape (profiling: a tuner timed under ncu is distorted)")
     ap.add_argument("--workload", default="walk-sgns", choices=["walk-sgns", "gcn"],
                     help="gcn: the offline common-neighbour tool instead of the walk + SGNS rounds")
+    ap.add_argument("--write-graph", default=None, help=argparse.SUPPRESS)
     args = ap.parse_args()
+    if args.write_graph:
+        # helper of the reference arm: the configuration's training edges as a
+        # 12-byte binary edge file, and its vertex count on stdout
+        g = make_graph(CONFIGS[args.config])
+        g["edges"].tofile(args.write_graph)
+        print(json.dumps({"v_num": g["v_num"]}))
+        return
     if args.workload == "gcn":
         bench_gcn(args)
     elif args.impl == "reference":

@@ -197,13 +197,18 @@ felog_status felog_get_alias(felog_ctx *ctx, float *prob, uint32_t *alias);
  * footprint after start-up).  It allocates nothing: inputs and outputs are the
  * caller's device buffers (row_ptr: v_num + 1 u64 CSR offsets; weight, prob,
  * alias: e_num entries) and its worklists live in a fixed device array of
- * FELOG_NOALLOC_MAX_ENTRIES entries that every GPU loading this library holds
- * until exit; larger graphs get FELOG_INVALID_ARG.  The first call on a device
- * (with that device current) looks the array up; make it before any stream
- * capture.  Calls share the array, so calls that overlap on the GPU race.
+ * FELOG_NOALLOC_MAX_ENTRIES entries (16 MiB) that a GPU holds, once mapped,
+ * until exit; larger graphs get FELOG_INVALID_ARG.  CUDA maps that array on a
+ * device lazily, at the first call there (with that device current): make
+ * one call at start-up, before the caller's own pool reserves the free memory
+ * and before any stream capture; a first call that finds no room returns
+ * FELOG_OOM.  Every call looks the array's address up again.  Calls share the
+ * array, so calls that overlap on the GPU race.
  * stream: a cudaStream_t, or NULL for the default stream; the call
  * synchronizes it.  Returns FELOG_INVALID_ARG for a null buffer, for more than
- * FELOG_NOALLOC_MAX_ENTRIES entries (before touching the device) and for a
+ * FELOG_NOALLOC_MAX_ENTRIES entries (before touching the device), for edges
+ * without vertices, for a vertex whose row_ptr range is out of order or ends
+ * past e_num (checked on the device before any worklist access) and for a
  * negative or non-finite weight; FELOG_CUDA_ERROR when a CUDA call fails. */
 #define FELOG_NOALLOC_MAX_ENTRIES (1ull << 22)
 felog_status felog_build_alias_noalloc(const uint64_t *row_ptr, const float *weight, uint32_t v_num,
@@ -289,6 +294,21 @@ felog_status felog_get_plan(felog_ctx *ctx, int32_t *sen, uint64_t *sent_start, 
 /* ---- budget ---- */
 felog_status felog_budget_check(felog_ctx *ctx, uint32_t round, felog_budget_stats *stats);
 felog_status felog_get_similarity(felog_ctx *ctx, float *sim);
+
+/* ---- classes ----
+ * -classes k output (src/word2vec.cu:2128-2175 writes one class id per
+ * vocabulary row): spherical K-means over the resident syn0 rows on the GPU.
+ * Objective: the sum over rows of row . centroid(label) for unit centroids;
+ * each iteration assigns every row to its largest-dot centroid (ties to the
+ * lower index) and then replaces every centroid by the normalised sum of its
+ * rows (an empty one keeps its value), so the objective never decreases.
+ * Seeds: the normalised rows at vocabulary positions floor((j + 0.5) V / k).
+ * Stops after max_iter assignment passes (0: 10) or at the first pass that
+ * changes no label.  labels (host, vocab_size entries, vocabulary order),
+ * objective (host, max_iter entries: the objective after each assignment
+ * pass) and iterations (passes run) are optional.  Deterministic. */
+felog_status felog_cluster_embeddings(felog_ctx *ctx, int32_t classes, int32_t max_iter, int32_t *labels,
+                                      double *objective, int32_t *iterations);
 
 /* ---- learned walk budget (no reference counterpart) ----
  * A 6 -> 64 -> 64 -> (9 + 1) MLP predicts each vertex's walk count (2..10)

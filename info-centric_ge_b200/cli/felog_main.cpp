@@ -83,45 +83,6 @@ bool validate_partition(const std::string &path, uint32_t v_num) {
   return t == 2 && b == 0;
 }
 
-// K-means over the rows as in word2vec.cu:2128-2175 (10 iterations, cosine assignment).
-void kmeans(const std::vector<float> &syn0, long long vocab, int dim, int classes, std::vector<int> &cl) {
-  int iter = 10;
-  std::vector<int> centcn(classes);
-  cl.assign(vocab, 0);
-  std::vector<float> cent((size_t)classes * dim);
-  for (long long a = 0; a < vocab; a++) cl[a] = (int)(a % classes);
-  for (int a = 0; a < iter; a++) {
-    std::fill(cent.begin(), cent.end(), 0.0f);
-    std::fill(centcn.begin(), centcn.end(), 1);
-    for (long long c = 0; c < vocab; c++) {
-      for (int d = 0; d < dim; d++) cent[(size_t)dim * cl[c] + d] += syn0[(size_t)c * dim + d];
-      centcn[cl[c]]++;
-    }
-    for (int b = 0; b < classes; b++) {
-      float closev = 0;
-      for (int c = 0; c < dim; c++) {
-        cent[(size_t)dim * b + c] /= centcn[b];
-        closev += cent[(size_t)dim * b + c] * cent[(size_t)dim * b + c];
-      }
-      closev = sqrtf(closev);
-      for (int c = 0; c < dim; c++) cent[(size_t)dim * b + c] /= closev;
-    }
-    for (long long c = 0; c < vocab; c++) {
-      float closev = -10;
-      int closeid = 0;
-      for (int d = 0; d < classes; d++) {
-        float x = 0;
-        for (int b = 0; b < dim; b++) x += cent[(size_t)dim * d + b] * syn0[(size_t)c * dim + b];
-        if (x > closev) {
-          closev = x;
-          closeid = d;
-        }
-      }
-      cl[c] = closeid;
-    }
-  }
-}
-
 }  // namespace
 
 int main(int argc, char **argv) {
@@ -258,14 +219,14 @@ int main(int argc, char **argv) {
   }
   if (!cli.emb_output.empty()) {
     if (o.classes > 0) {
+      // class ids from the GPU spherical K-means (10 passes at most)
       uint64_t vs = 0;
       felog_vocab_info(ctx, &vs, nullptr);
-      std::vector<float> s0(vs * (uint64_t)o.size);
       std::vector<uint32_t> vv(vs);
-      if (felog_get_embeddings(ctx, s0.data(), nullptr, s0.size()) != FELOG_OK) die("get_embeddings");
+      std::vector<int32_t> cl(vs);
       felog_get_vocab(ctx, vv.data(), nullptr);
-      std::vector<int> cl;
-      kmeans(s0, (long long)vs, o.size, o.classes, cl);
+      if (felog_cluster_embeddings(ctx, o.classes, 10, cl.data(), nullptr, nullptr) != FELOG_OK)
+        die("cluster_embeddings");
       FILE *f = fopen(cli.emb_output.c_str(), "wb");
       if (!f) die("emb_output");
       for (uint64_t a = 0; a < vs; a++) fprintf(f, "%u %d\n", vv[a], cl[a]);

@@ -19,6 +19,7 @@
 #include <vector>
 
 #include "budget.cuh"
+#include "cluster.cuh"
 #include "common.cuh"
 #include "gcn.cuh"
 #include "graph.cuh"
@@ -231,6 +232,15 @@ __global__ void k_to_host(const void *src, void *dst, uint64_t bytes) {
   const uint8_t *s = static_cast<const uint8_t *>(src);
   uint8_t *d = static_cast<uint8_t *>(dst);
   for (uint64_t i = body + t0; i < bytes; i += stride) d[i] = s[i];
+}
+
+// out += sum of x[0..n) (per-warp sums, one atomic per warp)
+__global__ void k_sum_u32(const uint32_t *__restrict__ x, uint64_t n, unsigned long long *out) {
+  unsigned long long t = 0;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    t += x[i];
+  for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+  if ((threadIdx.x & 31) == 0 && t) atomicAdd(out, t);
 }
 
 // Synchronous readback of `bytes` device bytes on the context's stream, through
@@ -1574,6 +1584,12 @@ extern "C" felog_status felog_train_round(felog_ctx *c, uint32_t round, float al
     CK(cudaGetLastError(), "train_round: launch");
   }
   CK(cudaEventRecord(c->ev1, c->stream), "train_round");
+  // words considered = sum of the plan's considered tokens per sentence (counter 2)
+  CK(cudaMemsetAsync(c->counters.p + 2, 0, 8, c->stream), "train_round");
+  if (c->plan_sent) {
+    k_sum_u32<<<grid_for(c, c->plan_sent, 256), 256, 0, c->stream>>>(c->p_cons.p, c->plan_sent, c->counters.p + 2);
+    c->launches++;
+  }
   unsigned long long h[4];
   RB(h, c->counters.p, sizeof h, "train_round");
   s = check_dev_err(c, "train_round");
@@ -1581,13 +1597,7 @@ extern "C" felog_status felog_train_round(felog_ctx *c, uint32_t round, float al
   CK(cudaEventElapsedTime(&ms_train, c->ev0, c->ev1), "train_round");
   if (stats) {
     memset(stats, 0, sizeof(*stats));
-    // words considered = sum of considered tokens per sentence
-    std::vector<uint32_t> cons(c->plan_sent);
-    if (c->plan_sent)
-      RB(cons.data(), c->p_cons.p, 4 * (size_t)c->plan_sent, "train_round");
-    uint64_t w = 0;
-    for (uint32_t x : cons) w += x;
-    stats->words = w;
+    stats->words = h[2];
     stats->kept_words = c->plan_sen;
     stats->pairs = h[1];
     stats->sentences = c->plan_sent;
@@ -1904,6 +1914,115 @@ extern "C" felog_status felog_get_similarity(felog_ctx *c, float *sim) {
   if (!c || !sim) return FELOG_INVALID_ARG;
   if (!c->model_ready) return fail(c, FELOG_NOT_READY, "model not initialised");
   CK(cudaMemcpy(sim, c->sim.p, 4 * (size_t)c->V, cudaMemcpyDeviceToHost), "get_similarity");
+  return FELOG_OK;
+}
+
+// ---------------------------------------------------------------- classes
+
+namespace {
+template <int D, class P>
+void km_launch(felog_ctx *c, KmArgs &a, int which, int blocks, const uint32_t *sorted, const uint64_t *seg) {
+  if (which == 0) k_km_seed<D, P><<<std::min(a.k, 4096), 32, 0, c->stream>>>(a);
+  else if (which == 1) k_km_assign<D, P><<<blocks, 256, 0, c->stream>>>(a);
+  else k_km_update<D, P><<<std::min(a.k, 65535), 256, 0, c->stream>>>(a, sorted, seg);
+  c->launches++;
+}
+template <class P>
+void km_dispatch(felog_ctx *c, KmArgs &a, int which, int blocks, const uint32_t *sorted, const uint64_t *seg) {
+  switch (c->o.size) {
+    case 32: km_launch<32, P>(c, a, which, blocks, sorted, seg); break;
+    case 64: km_launch<64, P>(c, a, which, blocks, sorted, seg); break;
+    case 128: km_launch<128, P>(c, a, which, blocks, sorted, seg); break;
+    case 256: km_launch<256, P>(c, a, which, blocks, sorted, seg); break;
+  }
+}
+}  // namespace
+
+extern "C" felog_status felog_cluster_embeddings(felog_ctx *c, int32_t classes, int32_t max_iter, int32_t *labels,
+                                                 double *objective, int32_t *iterations) {
+  if (!c) return FELOG_INVALID_ARG;
+  if (!c->model_ready) return fail(c, FELOG_NOT_READY, "model not initialised");
+  const uint64_t n = (uint64_t)c->vocab_size;
+  if (classes < 1 || (uint64_t)classes > n || classes > (1 << 24))
+    return fail(c, FELOG_INVALID_ARG, "cluster_embeddings: classes must be in [1, min(vocab, 2^24)]");
+  if (max_iter < 0) return fail(c, FELOG_INVALID_ARG, "cluster_embeddings: max_iter must be >= 0");
+  if (max_iter == 0) max_iter = 10;
+  if (n > 0xFFFFFFFFull) return fail(c, FELOG_INVALID_ARG, "cluster_embeddings: more than 2^32 rows");
+  CK(cudaSetDevice(c->device), "cluster_embeddings");
+  const int dim = c->o.size;
+  DevBuf<float> cent;
+  DevBuf<int32_t> lab;
+  DevBuf<double> part;
+  DevBuf<uint32_t> keys, vals, keys2, vals2;
+  DevBuf<unsigned long long> cnt;
+  DevBuf<uint64_t> seg;
+  const int blocks = grid_for(c, n * 32, 256, 8);
+  CK(cent.ensure((size_t)classes * dim), "cluster_embeddings");
+  CK(lab.ensure(n), "cluster_embeddings");
+  CK(part.ensure(blocks), "cluster_embeddings");
+  CK(keys.ensure(n), "cluster_embeddings");
+  CK(vals.ensure(n), "cluster_embeddings");
+  CK(keys2.ensure(n), "cluster_embeddings");
+  CK(vals2.ensure(n), "cluster_embeddings");
+  CK(cnt.ensure((size_t)classes + 1), "cluster_embeddings");
+  CK(seg.ensure((size_t)classes + 1), "cluster_embeddings");
+  KmArgs a{};
+  a.rows.syn0 = c->syn0.p;
+  a.rows.syn0_bf = c->syn0_bf.p;
+  a.rows.n_hot = c->n_f32;
+  a.n_rows = n;
+  a.k = classes;
+  a.cent = cent.p;
+  a.labels = lab.p;
+  a.obj_partial = part.p;
+  a.changed = c->counters.p;
+  const bool bf = c->o.precision == FELOG_BF16;
+  auto launch = [&](int which, const uint32_t *sorted, const uint64_t *sg) {
+    if (bf) km_dispatch<RowsBF16>(c, a, which, blocks, sorted, sg);
+    else km_dispatch<RowsF32>(c, a, which, blocks, sorted, sg);
+  };
+  launch(0, nullptr, nullptr);
+  CK(cudaGetLastError(), "cluster_embeddings: seed");
+  int end_bit = 1;
+  while (end_bit < 32 && (1ULL << end_bit) < (uint64_t)classes) end_bit++;
+  std::vector<double> hp(blocks);
+  int it = 0;
+  for (; it < max_iter; it++) {
+    a.first = it == 0;
+    CK(cudaMemsetAsync(c->counters.p, 0, sizeof(unsigned long long), c->stream), "cluster_embeddings");
+    launch(1, nullptr, nullptr);
+    CK(cudaGetLastError(), "cluster_embeddings: assign");
+    unsigned long long changed = 0;
+    RB(&changed, c->counters.p, sizeof changed, "cluster_embeddings");
+    RB(hp.data(), part.p, sizeof(double) * blocks, "cluster_embeddings");
+    double obj = 0.0;
+    for (int b = 0; b < blocks; b++) obj += hp[b];
+    if (objective) objective[it] = obj;
+    if (changed == 0) {
+      it++;
+      break;
+    }
+    // rows grouped by label (stable: ascending row index inside a label)
+    CK(cudaMemsetAsync(cnt.p, 0, sizeof(unsigned long long) * (classes + 1), c->stream), "cluster_embeddings");
+    k_km_count<<<grid_for(c, n, 256), 256, 0, c->stream>>>(lab.p, n, keys.p, vals.p, cnt.p);
+    c->launches++;
+    cub::DoubleBuffer<uint32_t> dk(keys.p, keys2.p), dv(vals.p, vals2.p);
+    size_t tmp = 0;
+    CK(cub::DeviceRadixSort::SortPairs(nullptr, tmp, dk, dv, (int)n, 0, end_bit, c->stream), "cluster_embeddings");
+    CK(c->cub_tmp.ensure(tmp), "cluster_embeddings");
+    CK(cub::DeviceRadixSort::SortPairs(c->cub_tmp.p, tmp, dk, dv, (int)n, 0, end_bit, c->stream),
+       "cluster_embeddings");
+    tmp = 0;
+    CK(cub::DeviceScan::ExclusiveSum(nullptr, tmp, cnt.p, (unsigned long long *)seg.p, classes + 1, c->stream),
+       "cluster_embeddings");
+    CK(c->cub_tmp.ensure(tmp), "cluster_embeddings");
+    CK(cub::DeviceScan::ExclusiveSum(c->cub_tmp.p, tmp, cnt.p, (unsigned long long *)seg.p, classes + 1, c->stream),
+       "cluster_embeddings");
+    launch(2, dv.Current(), seg.p);
+    CK(cudaGetLastError(), "cluster_embeddings: update");
+  }
+  if (iterations) *iterations = it;
+  if (labels) CK(cudaMemcpy(labels, lab.p, sizeof(int32_t) * n, cudaMemcpyDeviceToHost), "cluster_embeddings");
   return FELOG_OK;
 }
 

@@ -11,14 +11,21 @@
 // kNoAllocMaxEntries CSR entries (16 MiB of worklist words).  Every GPU that
 // loads this library holds that array until the process exits.
 //
-// Set-up: the first call on a device (with that device current) looks up the
-// array's device address with cudaGetSymbolAddress and caches it; make that
-// first call before any stream capture.  All calls share the one array and it
-// keeps the last call's contents; calls that overlap on the GPU (on different
-// streams, or from different threads) race on it, so callers serialise them.
+// Set-up: every call looks up the array's device address on the current
+// device with cudaGetSymbolAddress (nothing is cached, so a call after a
+// device reset sees the reloaded module).  With CUDA's lazy module loading
+// the array is mapped on a device by the first call there, not when the
+// library is loaded: make one call at start-up, before the caller's own pool
+// reserves the free memory, and before any stream capture.  A first call that
+// finds no room for the array returns FELOG_OOM.  All calls share the one
+// array and it keeps the last call's contents; calls that overlap on the GPU
+// (on different streams, or from different threads) race on it, so callers
+// serialise them.
+//
+// The kernel checks every vertex's CSR range against e_num before touching
+// the worklists, so a row_ptr that is out of order or points past e_num is
+// reported as FELOG_INVALID_ARG and never indexes past the array.
 #include <cuda_runtime.h>
-
-#include <mutex>
 
 #include "alias.cuh"
 #include "felog_gpu.h"
@@ -33,20 +40,25 @@ constexpr uint64_t kHeaderWords = 64;
 constexpr uint64_t kNoAllocMaxEntries = FELOG_NOALLOC_MAX_ENTRIES;
 static __device__ __align__(256) uint32_t g_alias_scratch[kHeaderWords + kNoAllocMaxEntries];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_setup_mu;
-uint32_t *g_scratch_ptr[kMaxDevices] = {nullptr};
+// device error code of a CSR range outside [0, e_num] or out of order
+constexpr int kErrBadRowPtr = 64;
 
 __global__ void k_build_alias_weights(const uint64_t *__restrict__ row_ptr, const float *__restrict__ weight_of,
-                                      uint32_t v_num, float *__restrict__ prob, uint32_t *__restrict__ alias,
-                                      uint32_t *__restrict__ scratch) {
+                                      uint32_t v_num, uint64_t e_num, float *__restrict__ prob,
+                                      uint32_t *__restrict__ alias, uint32_t *__restrict__ scratch) {
   uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
   int *err = reinterpret_cast<int *>(scratch);
   uint32_t *work = scratch + kHeaderWords;
   auto weight = [weight_of](uint64_t j) { return weight_of[j]; };
-  for (uint32_t v = warp; v < v_num; v += nwarps)
-    alias_build_vertex(row_ptr[v], row_ptr[v + 1], weight, prob, alias, work, err);
+  for (uint32_t v = warp; v < v_num; v += nwarps) {
+    const uint64_t b = row_ptr[v], e = row_ptr[v + 1];
+    if (e < b || e > e_num || e - b > 0xFFFFFFFFull) {
+      if (lane_id() == 0) set_error(err, kErrBadRowPtr);
+      continue;  // uniform across the warp: b and e are the same in every lane
+    }
+    alias_build_vertex(b, e, weight, prob, alias, work, err);
+  }
 }
 
 }  // namespace
@@ -55,36 +67,37 @@ extern "C" felog_status felog_build_alias_noalloc(const uint64_t *d_row_ptr, con
                                                  uint32_t v_num, uint64_t e_num, float *d_prob,
                                                  uint32_t *d_alias, void *stream) {
   // status codes: FELOG_INVALID_ARG for a null buffer, more than
-  // FELOG_NOALLOC_MAX_ENTRIES entries (rejected before any device work) or a
-  // negative / non-finite weight; FELOG_CUDA_ERROR for a failed CUDA call.
+  // FELOG_NOALLOC_MAX_ENTRIES entries (rejected before any device work), edges
+  // without vertices, a CSR range outside [0, e_num] or a negative /
+  // non-finite weight; FELOG_OOM when the array cannot be mapped on this
+  // device; FELOG_CUDA_ERROR for a failed CUDA call.
   if (!d_row_ptr || (e_num && (!d_weight || !d_prob || !d_alias))) return FELOG_INVALID_ARG;
   if (e_num > kNoAllocMaxEntries) return FELOG_INVALID_ARG;
+  if (v_num == 0) return e_num ? FELOG_INVALID_ARG : FELOG_OK;
   int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return FELOG_CUDA_ERROR;
-  uint32_t *scratch;
-  {
-    std::lock_guard<std::mutex> g(g_setup_mu);
-    if (!g_scratch_ptr[dev]) {
-      // a host-side use of g_alias_scratch names a host shadow, not device memory
-      void *p = nullptr;
-      if (cudaGetSymbolAddress(&p, g_alias_scratch) != cudaSuccess) return FELOG_CUDA_ERROR;
-      g_scratch_ptr[dev] = static_cast<uint32_t *>(p);
-    }
-    scratch = g_scratch_ptr[dev];
+  if (cudaGetDevice(&dev) != cudaSuccess) return FELOG_CUDA_ERROR;
+  // host code must not hand g_alias_scratch itself to a kernel: on the host
+  // that name is a shadow variable, not device memory
+  void *p = nullptr;
+  const cudaError_t ge = cudaGetSymbolAddress(&p, g_alias_scratch);
+  if (ge != cudaSuccess) {
+    cudaGetLastError();
+    return ge == cudaErrorMemoryAllocation ? FELOG_OOM : FELOG_CUDA_ERROR;
   }
-  if (v_num == 0 || e_num == 0) return FELOG_OK;
+  uint32_t *scratch = static_cast<uint32_t *>(p);
+  if (e_num == 0) return FELOG_OK;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   if (cudaMemsetAsync(scratch, 0, sizeof(uint32_t), st) != cudaSuccess) return FELOG_CUDA_ERROR;
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   uint64_t want = ((uint64_t)v_num * 32 + 255) / 256;
   int blocks = (int)(want < (uint64_t)sms * 8 ? (want ? want : 1) : (uint64_t)sms * 8);
-  k_build_alias_weights<<<blocks, 256, 0, st>>>(d_row_ptr, d_weight, v_num, d_prob, d_alias, scratch);
+  k_build_alias_weights<<<blocks, 256, 0, st>>>(d_row_ptr, d_weight, v_num, e_num, d_prob, d_alias, scratch);
   if (cudaGetLastError() != cudaSuccess) return FELOG_CUDA_ERROR;
   int h = 0;
   cudaError_t e = cudaMemcpyAsync(&h, scratch, sizeof(int), cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) return FELOG_CUDA_ERROR;
-  if (h == kErrBadWeight) return FELOG_INVALID_ARG;
+  if (h == kErrBadWeight || h == kErrBadRowPtr) return FELOG_INVALID_ARG;
   return h == 0 ? FELOG_OK : FELOG_INTERNAL;
 }

@@ -164,6 +164,7 @@ def gpu_lib():
         L.felog_get_plan.argtypes = [_P, _P, _P, _P, _P]
         L.felog_budget_check.argtypes = [_P, ctypes.c_uint32, ctypes.POINTER(BudgetStats)]
         L.felog_get_similarity.argtypes = [_P, _P]
+        L.felog_cluster_embeddings.argtypes = [_P, ctypes.c_int32, ctypes.c_int32, _P, _P, _P]
         L.felog_run.argtypes = [_P, ctypes.POINTER(RunStats)]
         L.felog_write_embeddings.argtypes = [_P, ctypes.c_char_p]
         L.felog_kernel_launches.argtypes = [_P]
@@ -473,6 +474,19 @@ class Felog:
         self._ck(self._L.felog_get_similarity(self.h, _addr(s)))
         return s
 
+    def cluster(self, classes, max_iter=10):
+        """Spherical K-means over syn0 on the GPU (the -classes output).
+
+        Returns (labels per vocabulary row, objective after each assignment pass)."""
+        n = ctypes.c_uint64()
+        self._ck(self._L.felog_vocab_info(self.h, ctypes.byref(n), None))
+        lab = np.zeros(n.value, np.int32)
+        obj = np.zeros(max(max_iter, 1) if max_iter else 10, np.float64)
+        it = ctypes.c_int32()
+        self._ck(self._L.felog_cluster_embeddings(self.h, classes, max_iter, _addr(lab), _addr(obj),
+                                                  ctypes.byref(it)))
+        return lab, obj[: it.value]
+
     # ---- loop
     def run(self):
         st = RunStats()
@@ -549,10 +563,17 @@ def synth_graph(seed, v_target, e_target, abcd=(0.57, 0.19, 0.19, 0.05), lognorm
                 info=_struct_dict(info))
 
 
+NOALLOC_MAX_ENTRIES = 1 << 22  # FELOG_NOALLOC_MAX_ENTRIES
+
+
 def build_alias_noalloc(row_ptr_dev, weight_dev, v_num, e_num, prob_dev, alias_dev, stream=None):
     """felog_build_alias_noalloc on caller-owned device buffers (integer device addresses).
 
     For callers that cannot allocate device memory; raises FelogError on failure."""
+    if not 0 < v_num < 2 ** 32:
+        raise FelogError(1, f"v_num {v_num} outside [1, 2^32)")
+    if not 0 <= e_num <= NOALLOC_MAX_ENTRIES:
+        raise FelogError(1, f"e_num {e_num} outside [0, {NOALLOC_MAX_ENTRIES}]")
     L = gpu_lib()
     st = L.felog_build_alias_noalloc(row_ptr_dev, weight_dev, v_num, e_num, prob_dev, alias_dev, stream)
     if st != 0:

@@ -1,7 +1,8 @@
 """Regenerates the golden fixtures under tests/golden/ from the reference.
 
-Needs the reference checkout (REF, default /root/reference) and the harness
-binaries built by ``make -C oracle ref`` (oracle/_ref/).  Every fixture is the
+Needs the harness
+binaries built by ``make -C oracle ref`` (oracle/_ref/) from the reference
+checkout that FELOG_REFERENCE names.  Every fixture is the
 reference's own output on seeded synthetic inputs:
 
   walk_*.npz   include/walk.hpp run by oracle/_ref/ref_walk with injected draws:

@@ -8,7 +8,8 @@ through the C ABI twice in a row (the second call reuses the array the first
 one left behind) and compares both results with felog_build_alias on the same
 graph.  The tables are deterministic, so the comparison is exact.  The device
 buffers of the test itself come from torch: the test plays the caller, and the
-entry point allocates nothing.
+entry point allocates nothing, which the test checks by reading the device's
+free memory around the second call.
 """
 import ctypes
 
@@ -43,8 +44,12 @@ def test_noalloc_alias_matches_allocating_entry_point_twice():
         d_prob = torch.full((M,), -1.0, dtype=torch.float32, device=dev)
         d_alias = torch.full((M,), -1, dtype=torch.int32, device=dev)
         torch.cuda.synchronize()
+        free_before = torch.cuda.mem_get_info(dev)[0]
         fb.build_alias_noalloc(d_row.data_ptr(), d_w.data_ptr(), V, M, d_prob.data_ptr(), d_alias.data_ptr())
         torch.cuda.synchronize()
+        if call == 1:
+            # the first call may map the fixed array; the second one changes nothing
+            assert torch.cuda.mem_get_info(dev)[0] == free_before
         np.testing.assert_array_equal(d_prob.cpu().numpy(), prob_ref, err_msg=f"call {call}")
         np.testing.assert_array_equal(d_alias.cpu().numpy().view(np.uint32), alias_ref, err_msg=f"call {call}")
     f.close()
@@ -69,3 +74,27 @@ def test_noalloc_alias_rejects_oversized_graphs_and_bad_weights():
     # the error word is cleared by the next call
     w[1] = 2.0
     fb.build_alias_noalloc(row.data_ptr(), w.data_ptr(), 2, 3, prob.data_ptr(), alias.data_ptr())
+
+
+def test_noalloc_alias_rejects_inconsistent_row_ptr():
+    import torch
+
+    dev = torch.device("cuda:0")
+    # vertex 1's range ends past e_num (5 > 4), vertex 2's range runs backwards;
+    # every buffer is large enough for the offsets, so the test itself never
+    # writes out of bounds
+    row = torch.tensor([0, 2, 5, 3], dtype=torch.int64, device=dev)
+    w = torch.ones(8, dtype=torch.float32, device=dev)
+    prob = torch.zeros(8, dtype=torch.float32, device=dev)
+    alias = torch.zeros(8, dtype=torch.int32, device=dev)
+    with pytest.raises(fb.FelogError) as ei:
+        fb.build_alias_noalloc(row.data_ptr(), w.data_ptr(), 3, 4, prob.data_ptr(), alias.data_ptr())
+    assert ei.value.status == 1
+    L = fb.gpu_lib()
+    assert L.felog_build_alias_noalloc(row.data_ptr(), w.data_ptr(), 0, 4, prob.data_ptr(), alias.data_ptr(),
+                                       None) == 1  # edges without vertices
+    # a consistent CSR over the same buffers succeeds afterwards
+    row2 = torch.tensor([0, 2, 3, 4], dtype=torch.int64, device=dev)
+    fb.build_alias_noalloc(row2.data_ptr(), w.data_ptr(), 3, 4, prob.data_ptr(), alias.data_ptr())
+    torch.cuda.synchronize()
+    assert torch.all(prob[:4] == 1.0)
