@@ -103,6 +103,8 @@ struct felog_ctx {
   uint64_t n_sent = 0, n_tok = 0;
   uint64_t last_walk_tokens = 0, last_walk_traces = 0;  // totals of the last walk round
   uint64_t last_chunk_pairs = 0;  // pair records of the last trained chunk (still in pr_rec)
+  uint64_t round_stream_pairs = 0;  // pairs of the round's pair stream (the pair trainer counts none itself)
+  bool round_used_stream = false;
   int last_chunk_stride = 0;
   bool corpus_ready = false;
   DevBuf<unsigned int> visit_freq;
@@ -1369,6 +1371,7 @@ felog_status train_pairs(felog_ctx *c, SgArgs g, int blocks, int threads) {
   pa.cfirst = c->pr_cfirst.p;
   pa.reuse = c->o.reuse_neg ? 1 : 0;
   pa.coarse = c->table_coarse.p;
+  pa.sr_seed = g.sr_seed;
   pa.negs = c->p_negs.p;
   pa.count = c->pr_count.p;
   pa.off = c->pr_off.p;
@@ -1384,6 +1387,8 @@ felog_status train_pairs(felog_ctx *c, SgArgs g, int blocks, int threads) {
      "train");
   uint64_t total = 0;
   RB(&total, c->pr_off.p + n, 8, "train");
+  c->round_stream_pairs = total;
+  c->round_used_stream = true;
   // chunks of whole sentences
   std::vector<std::pair<uint64_t, uint64_t>> chunks;
   if (total <= kPairChunk) {
@@ -1506,6 +1511,7 @@ extern "C" felog_status felog_train_round(felog_ctx *c, uint32_t round, float al
   CK(cudaMemsetAsync(c->counters.p, 0, sizeof(unsigned long long) * 16, c->stream), "train_round");
   CK(cudaMemsetAsync(c->derr.p, 0, sizeof(int), c->stream), "train_round");
   c->last_chunk_pairs = 0;  // set again if this round trains over the pair stream
+  c->round_used_stream = false;
   felog_status s = plan_round(c, &ms_plan);
   if (s != FELOG_OK) return s;
   CK(cudaMemsetAsync(c->counters.p, 0, sizeof(unsigned long long) * 4, c->stream), "train_round");
@@ -1599,7 +1605,7 @@ extern "C" felog_status felog_train_round(felog_ctx *c, uint32_t round, float al
     memset(stats, 0, sizeof(*stats));
     stats->words = h[2];
     stats->kept_words = c->plan_sen;
-    stats->pairs = h[1];
+    stats->pairs = c->round_used_stream ? c->round_stream_pairs : h[1];
     stats->sentences = c->plan_sent;
     stats->batches = c->plan_batches;
     stats->alpha = alpha;

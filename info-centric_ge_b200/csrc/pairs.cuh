@@ -16,8 +16,9 @@
 // row work only.
 //
 // Record of one pair (int32 x stride, stride = K + 3 rounded up to 4):
-//   [0] context row, [1] positive target, [2 .. K+1] negatives (-1: skipped),
-//   [K+2] flags: bit 0 = two non-skipped negatives hit the same row.
+//   [0] context row, top bit set when two non-skipped negatives hit the same
+//       row, [1] positive target, [2 .. K+1] negatives (-1: skipped),
+//   [K+2] the pair's rounding key pair_key(seed, sentence, pair) (sgns.cuh).
 #pragma once
 
 #include "common.cuh"
@@ -25,7 +26,7 @@
 
 namespace felog {
 
-constexpr uint32_t kPairDup = 1u;
+constexpr uint32_t kPairDup = 0x80000000u;  // in word 0, over the context row
 
 __host__ __device__ constexpr int pair_stride(int negative) { return (negative + 3 + 3) & ~3; }
 
@@ -50,6 +51,7 @@ struct PairArgs {
   int reuse;             // -reuse-neg 1: full window, negatives from negs
   const int32_t *negs;   // plan negatives, K per sentence
   const uint32_t *coarse;  // per 64-slot bucket of the unigram table (see k_unigram_coarse)
+  uint32_t sr_seed;        // rounding seed of the round (the pair's key goes into its record)
 };
 
 // The unigram table is nondecreasing (word2vec.cu:683-690), so a bucket of 64
@@ -188,7 +190,6 @@ __global__ void __launch_bounds__(256) k_pair_emit(PairArgs a) {
         if (!live[u]) continue;
         uint32_t flags = 0;
         int32_t rv[S];
-        rv[0] = ctx[u];
         rv[1] = word[u];
 #pragma unroll
         for (int q = 0; q < K; q++) {
@@ -199,7 +200,8 @@ __global__ void __launch_bounds__(256) k_pair_emit(PairArgs a) {
           for (int q2 = 0; q2 < q; q2++) flags |= (v >= 0 && rv[2 + q2] == v) ? kPairDup : 0u;
           rv[2 + q] = v;
         }
-        rv[2 + K] = (int32_t)flags;
+        rv[0] = (int32_t)((uint32_t)ctx[u] | flags);
+        rv[2 + K] = (int32_t)pair_key(a.sr_seed, s, (uint32_t)(p0 + lane + 32 * u));
 #pragma unroll
         for (int q = K + 3; q < S; q++) rv[q] = 0;
         int4 *dst = reinterpret_cast<int4 *>(r0 + (p0 + lane + 32 * u) * S);
@@ -255,9 +257,10 @@ struct LaneRows {
 
   // row += u.  FP32 rows: vector reduction (cur unchanged, returns false).
   // BF16 rows: cur becomes SR(cur + u), stored with a plain store (returns true).
+  // x: the lane's mixed rounding key (lane_mix), slot: the row slot
   template <int W>
-  __device__ __forceinline__ bool update(uint32_t row, const float2 (&u)[H], float2 (&cur)[H],
-                                         uint32_t stream) const {
+  __device__ __forceinline__ bool update(uint32_t row, const float2 (&u)[H], float2 (&cur)[H], uint32_t x,
+                                         uint32_t slot) const {
     float *pf = const_cast<float *>(f[W]) + (size_t)row * DIM;
     if constexpr (!P::kBF16) {
       red_f32x2(pf, u);
@@ -268,7 +271,7 @@ struct LaneRows {
 #pragma unroll
       for (int k = 0; k < H; k++) {
         const float2 nv = __fadd2_rn(cur[k], u[k]);
-        w[k] = sr_bf16x2(nv.y, nv.x, sr_word(stream));
+        w[k] = sr_bf16x2(nv.y, nv.x, sr_bits(x, slot, (uint32_t)k));
       }
       if (hot) {
         red_f32x2(pf, u);
@@ -381,7 +384,8 @@ __device__ __forceinline__ int rec_at(const int4 (&v)[S / 4], int i) {
 // skip_gram_kernel semantics (word2vec.cu:442-536, hs = 0) over the pair
 // stream: one warp per sentence, the sentence's pairs in order.  The record of
 // the next pair is loaded one pair ahead (every lane reads the same 16-byte
-// words: one broadcast request).  With distinct targets the K + 1 scores come
+// words: one broadcast request).  The pair count of the chunk is known on the
+// host, so the kernel counts nothing.  With distinct targets the K + 1 scores come
 // from one multi_dot and each lane evaluates one gradient; a pair whose
 // negatives repeat a row takes the sequential path, where the later target
 // sees the earlier update as in the reference.
@@ -401,28 +405,29 @@ __global__ void __launch_bounds__(256, MINB)
   const int lane = lane_id();
   LaneRows<DIM, P> rows;
   rows.init(a);
-  unsigned long long my_pairs = 0;
   unsigned long long sc;
   while (claim_sentence(a, sc)) {
     const uint64_t gs = s0 + sc;  // sentence index in the round's plan
-    const uint64_t pb = off[gs] - base, pe = off[gs + 1] - base;
+    // pair indices relative to the chunk (a chunk holds at most 2^27 pairs)
+    const uint32_t pb = (uint32_t)(off[gs] - base), pe = (uint32_t)(off[gs + 1] - base);
     if (pb == pe) continue;
     int4 nxt[S / 4];
 #pragma unroll
-    for (int k = 0; k < S / 4; k++) nxt[k] = __ldg(reinterpret_cast<const int4 *>(rec + pb * S) + k);
-    for (uint64_t p = pb; p < pe; p++) {
+    for (int k = 0; k < S / 4; k++) nxt[k] = __ldg(reinterpret_cast<const int4 *>(rec + (size_t)pb * S) + k);
+    for (uint32_t p = pb; p < pe; p++) {
       int4 cur[S / 4];
 #pragma unroll
       for (int k = 0; k < S / 4; k++) cur[k] = nxt[k];
       if (p + 1 < pe) {
 #pragma unroll
-        for (int k = 0; k < S / 4; k++) nxt[k] = __ldg(reinterpret_cast<const int4 *>(rec + (p + 1) * S) + k);
+        for (int k = 0; k < S / 4; k++) nxt[k] = __ldg(reinterpret_cast<const int4 *>(rec + (size_t)(p + 1) * S) + k);
       }
-      const uint32_t l1 = (uint32_t)rec_at<S>(cur, 0);
+      const uint32_t r0 = (uint32_t)rec_at<S>(cur, 0);
+      const uint32_t l1 = r0 & ~kPairDup;
       int tg[NT];
 #pragma unroll
       for (int q = 0; q < NT; q++) tg[q] = rec_at<S>(cur, 1 + q);
-      const bool dup = (rec_at<S>(cur, NK + 2) & kPairDup) != 0;
+      const bool dup = (r0 & kPairDup) != 0;
       float2 x[H];
       rows.template load<0>(l1, x);
       float2 y[NT][H];
@@ -432,7 +437,7 @@ __global__ void __launch_bounds__(256, MINB)
       float2 neu[H];
 #pragma unroll
       for (int k = 0; k < H; k++) neu[k] = make_float2(0.0f, 0.0f);
-      const uint32_t key = P::kBF16 ? lane_key(a.sr_seed, gs, (uint32_t)(p - pb), lane) : 0u;
+      const uint32_t key = P::kBF16 ? lane_mix((uint32_t)rec_at<S>(cur, NK + 2), lane) : 0u;
       bool done = false;
       if constexpr (kMulti) {
         if (!dup) {
@@ -450,7 +455,7 @@ __global__ void __launch_bounds__(256, MINB)
               neu[k] = __ffma2_rn(g2, y[q][k], neu[k]);
               upd[k] = __fmul2_rn(g2, x[k]);
             }
-            rows.template update<1>((uint32_t)tg[q], upd, y[q], slot_stream(key, q));
+            rows.template update<1>((uint32_t)tg[q], upd, y[q], key, (uint32_t)q);
           }
           done = true;
         }
@@ -468,7 +473,7 @@ __global__ void __launch_bounds__(256, MINB)
             neu[k] = __ffma2_rn(g2, y[q][k], neu[k]);
             upd[k] = __fmul2_rn(g2, x[k]);
           }
-          const bool stored = rows.template update<1>((uint32_t)tg[q], upd, y[q], slot_stream(key, q));
+          const bool stored = rows.template update<1>((uint32_t)tg[q], upd, y[q], key, (uint32_t)q);
 #pragma unroll
           for (int r = q + 1; r < NT; r++)
             if (tg[r] == tg[q])
@@ -476,11 +481,9 @@ __global__ void __launch_bounds__(256, MINB)
               for (int k = 0; k < H; k++) y[r][k] = stored ? y[q][k] : __fadd2_rn(y[q][k], upd[k]);
         }
       }
-      rows.template update<0>(l1, neu, x, slot_stream(key, kSlotCtx));
-      my_pairs++;
+      rows.template update<0>(l1, neu, x, key, kSlotCtx);
     }
   }
-  if (lane == 0 && my_pairs) atomicAdd(a.pairs, my_pairs);
 }
 
 // -reuse-neg 2: __sgNegReuse's work (word2vec.cu:368-440: full window, the
@@ -531,7 +534,7 @@ __global__ void __launch_bounds__(256, 4) k_sgns_reuse_tile(SgArgs a) {
         if (tg[q] >= 0) rows.template load<1>((uint32_t)tg[q], y[q]);
       }
       const uint32_t center = (uint32_t)(pos - sb);
-      const uint32_t key = P::kBF16 ? lane_key(a.sr_seed, s, center, lane) : 0u;
+      const uint32_t key = P::kBF16 ? lane_mix(pair_key(a.sr_seed, s, center), lane) : 0u;
       const int tq = butterfly_target(lane);
       uint32_t vmask = 0;
 #pragma unroll
@@ -558,7 +561,7 @@ __global__ void __launch_bounds__(256, 4) k_sgns_reuse_tile(SgArgs a) {
             dy[q][k] = __ffma2_rn(g2, x[k], dy[q][k]);
           }
         }
-        rows.template update<0>(l1, neu, x, slot_stream(key, kSlotCtx + (uint32_t)(c - pos + a.window)));
+        rows.template update<0>(l1, neu, x, key, kSlotCtx + (uint32_t)(c - pos + a.window));
         my_pairs++;
       }
       // targets: a repeated negative adds its sum into the first occurrence
@@ -576,7 +579,7 @@ __global__ void __launch_bounds__(256, 4) k_sgns_reuse_tile(SgArgs a) {
       }
 #pragma unroll
       for (int q = 0; q < NT; q++)
-        if (tg[q] >= 0) rows.template update<1>((uint32_t)tg[q], dy[q], y[q], slot_stream(key, (uint32_t)q));
+        if (tg[q] >= 0) rows.template update<1>((uint32_t)tg[q], dy[q], y[q], key, (uint32_t)q);
     }
   }
   if (lane == 0 && my_pairs) atomicAdd(a.pairs, my_pairs);
@@ -735,7 +738,7 @@ __global__ void __launch_bounds__(32 * kTileWarps) k_sgns_reuse_tile_tc(SgArgs a
       }
       __syncwarp();
       const uint32_t center = (uint32_t)(pos - sb);
-      const uint32_t key = lane_key(a.sr_seed, s, center, lane);
+      const uint32_t key = lane_mix(pair_key(a.sr_seed, s, center), lane);
       float2 dy[NT][H];
 #pragma unroll
       for (int q = 0; q < NT; q++)
@@ -765,7 +768,7 @@ __global__ void __launch_bounds__(32 * kTileWarps) k_sgns_reuse_tile_tc(SgArgs a
         if (sm.first[i] == i) {
           const uint32_t w = (uint32_t)sm.word[i];
           const long long c = c0 + i + (c0 + i >= pos ? 1 : 0);
-          rows.template update<0>(w, neu, xs, slot_stream(key, kSlotCtx + (uint32_t)(c - pos + a.window)));
+          rows.template update<0>(w, neu, xs, key, kSlotCtx + (uint32_t)(c - pos + a.window));
         }
         my_pairs++;
       }
@@ -784,7 +787,7 @@ __global__ void __launch_bounds__(32 * kTileWarps) k_sgns_reuse_tile_tc(SgArgs a
       }
 #pragma unroll
       for (int q = 0; q < NT; q++)
-        if (tg[q] >= 0) rows.template update<1>((uint32_t)tg[q], dy[q], y[q], slot_stream(key, (uint32_t)q));
+        if (tg[q] >= 0) rows.template update<1>((uint32_t)tg[q], dy[q], y[q], key, (uint32_t)q);
       __syncwarp();
     }
   }
@@ -801,7 +804,7 @@ __global__ void k_pair_row_mix(const int32_t *__restrict__ rec, uint64_t n, int 
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
     const int32_t *r = rec + i * (uint64_t)stride;
     refs++;
-    hot += (uint32_t)r[0] < n_hot;
+    hot += ((uint32_t)r[0] & ~kPairDup) < n_hot;
     for (int q = 0; q < nt; q++) {
       const int32_t t = r[1 + q];
       refs += t >= 0;

@@ -130,24 +130,24 @@ __host__ __device__ __forceinline__ uint32_t sr_hash(uint32_t x) {
   return x;
 }
 
-// Rounding streams.  One hash per (sentence, pair, lane) gives the lane's key;
-// the stream of row slot `slot` (target index d = 0..K for syn1 rows,
-// kSlotCtx (+ window position for CBOW) for syn0 rows) starts at
-// key + slot * 0x27D4EB2F and takes one LCG step per two values: the new
-// state x gives its low 16 bits to the lane's value 2k and its high 16 bits to
-// value 2k + 1.  The start is hashed and a stream runs at most four steps, so
-// every value's 16 bits are uniform and each rounding is unbiased; the streams
-// depend on (seed, sentence, pair, slot, lane) only.
+// Rounding bits.  One hash per (sentence, pair) gives the pair's key
+// kp = H(seed ^ (s * 0x9E3779B1 + pair * 0x85EBCA77)); lane L mixes it to
+// x = kp ^ (L * 0xC2B2AE3D).  Word k (two values) of row slot `slot` (target
+// index d = 0..K for syn1 rows, kSlotCtx (+ window position for CBOW) for
+// syn0 rows) takes the bits (x + slot * 0x27D4EB2F + k * 0x165667B1) *
+// 0x9E3779B1 mod 2^32: the low 16 bits round the lane's value 2k, the high 16
+// bits value 2k + 1.  kp is uniform, so every value's 16 bits are uniform and
+// each rounding is unbiased; the bits depend on (seed, sentence, pair, slot,
+// lane) only.  A word costs one multiply-add once x is known, so a kernel
+// short of registers recomputes bits cheaply (the pair trainer reads kp from
+// its pair record instead of hashing).
 constexpr uint32_t kSlotCtx = 256;
-__host__ __device__ __forceinline__ uint32_t lane_key(uint32_t seed, uint64_t s, uint32_t pair, uint32_t lane) {
-  return sr_hash(seed ^ ((uint32_t)s * 0x9E3779B1u + pair * 0x85EBCA77u + lane * 0xC2B2AE3Du));
+__host__ __device__ __forceinline__ uint32_t pair_key(uint32_t seed, uint64_t s, uint32_t pair) {
+  return sr_hash(seed ^ ((uint32_t)s * 0x9E3779B1u + pair * 0x85EBCA77u));
 }
-__host__ __device__ __forceinline__ uint32_t slot_stream(uint32_t key, uint32_t slot) {
-  return key + slot * 0x27D4EB2Fu;
-}
-__device__ __forceinline__ uint32_t sr_word(uint32_t &st) {
-  st = st * 1664525u + 1013904223u;
-  return st;
+__host__ __device__ __forceinline__ uint32_t lane_mix(uint32_t kp, uint32_t lane) { return kp ^ (lane * 0xC2B2AE3Du); }
+__host__ __device__ __forceinline__ uint32_t sr_bits(uint32_t x, uint32_t slot, uint32_t k) {
+  return (x + slot * 0x27D4EB2Fu + k * 0x165667B1u) * 0x9E3779B1u;
 }
 // Two FP32 values to packed BF16 by stochastic rounding in one instruction
 // (sm_100a cvt.rs): hi goes to the upper half with random bits r >> 16, lo to
@@ -205,7 +205,7 @@ __device__ __forceinline__ void row_load(const SgArgs &a, int which, long long r
 // stored value SR(cur + u) (plain store), returns true.
 template <int DIM, class P>
 __device__ __forceinline__ bool row_update(const SgArgs &a, int which, long long row, const float (&u)[DIM / 32],
-                                           float (&cur)[DIM / 32], uint32_t stream) {
+                                           float (&cur)[DIM / 32], uint32_t x, uint32_t slot) {
   constexpr int J = DIM / 32;
   const int lane = lane_id();
   if constexpr (P::kBF16) {
@@ -216,7 +216,7 @@ __device__ __forceinline__ bool row_update(const SgArgs &a, int which, long long
       for (int k = 0; k < W; k++) {
         const float lo = __fadd_rn(cur[2 * k], u[2 * k]);
         const float hi = 2 * k + 1 < J ? __fadd_rn(cur[2 * k + 1], u[2 * k + 1]) : 0.0f;
-        w[k] = sr_bf16x2(hi, lo, sr_word(stream));
+        w[k] = sr_bf16x2(hi, lo, sr_bits(x, slot, (uint32_t)k));
         cur[2 * k] = bf16_lo(w[k]);
         if (2 * k + 1 < J) cur[2 * k + 1] = bf16_hi(w[k]);
       }
@@ -359,7 +359,7 @@ __global__ void __launch_bounds__(256) k_sgns_skipgram_any(SgArgs a) {
         const long long c = pos - a.window + aa;
         if (c < sb || c >= se) continue;
         const int l1 = a.sen[c];
-        const uint32_t key = P::kBF16 ? lane_key(a.sr_seed, s, pair, lane_id()) : 0u;
+        const uint32_t key = P::kBF16 ? lane_mix(pair_key(a.sr_seed, s, pair), lane_id()) : 0u;
         float x[J];
         row_load<DIM, P>(a, 0, l1, x);
         float neu[J];
@@ -404,7 +404,7 @@ __global__ void __launch_bounds__(256) k_sgns_skipgram_any(SgArgs a) {
               neu[j] = __fmaf_rn(g, y[q][j], neu[j]);
               upd[j] = __fmul_rn(g, x[j]);
             }
-            const bool stored = row_update<DIM, P>(a, 1, tg[q], upd, y[q], slot_stream(key, d0 + q));
+            const bool stored = row_update<DIM, P>(a, 1, tg[q], upd, y[q], key, d0 + q);
             // a later target with the same row sees this update
 #pragma unroll
             for (int r = q + 1; r < kChunk; r++)
@@ -413,7 +413,7 @@ __global__ void __launch_bounds__(256) k_sgns_skipgram_any(SgArgs a) {
                 for (int j = 0; j < J; j++) y[r][j] = stored ? y[q][j] : __fadd_rn(y[q][j], upd[j]);
           }
         }
-        row_update<DIM, P>(a, 0, l1, neu, x, slot_stream(key, kSlotCtx));
+        row_update<DIM, P>(a, 0, l1, neu, x, key, kSlotCtx);
       }
     }
   }
@@ -437,7 +437,7 @@ __global__ void __launch_bounds__(256) k_sgns_cbow(SgArgs a) {
     unsigned long long nr = a.blk[s];
     for (long long pos = sb; pos < se; pos++) {
       const int word = a.sen[pos];
-      const uint32_t key = P::kBF16 ? lane_key(a.sr_seed, s, (uint32_t)(pos - sb), lane_id()) : 0u;
+      const uint32_t key = P::kBF16 ? lane_mix(pair_key(a.sr_seed, s, (uint32_t)(pos - sb)), lane_id()) : 0u;
       nr = nr * 2514903917ULL + 11ULL;
       const int b = (int)(nr % (unsigned long long)a.window);
       float neu1[J], neu1e[J];
@@ -494,7 +494,7 @@ __global__ void __launch_bounds__(256) k_sgns_cbow(SgArgs a) {
             neu1e[j] = __fmaf_rn(g, y[q][j], neu1e[j]);
             upd[j] = __fmul_rn(g, neu1[j]);
           }
-          const bool stored = row_update<DIM, P>(a, 1, tg[q], upd, y[q], slot_stream(key, d0 + q));
+          const bool stored = row_update<DIM, P>(a, 1, tg[q], upd, y[q], key, d0 + q);
 #pragma unroll
           for (int r = q + 1; r < kChunk; r++)
             if (tg[r] == tg[q])
@@ -510,7 +510,7 @@ __global__ void __launch_bounds__(256) k_sgns_cbow(SgArgs a) {
         if (c < sb || c >= se) continue;
         float x[J];
         if constexpr (P::kBF16) row_load<DIM, P>(a, 0, a.sen[c], x);
-        row_update<DIM, P>(a, 0, a.sen[c], neu1e, x, slot_stream(key, kSlotCtx + aa));
+        row_update<DIM, P>(a, 0, a.sen[c], neu1e, x, key, kSlotCtx + aa);
       }
     }
   }

@@ -555,12 +555,12 @@ void orc_cbow_batch(float *syn0, float *syn1, const float *exp_table, const int3
  * counterpart).  Rows 0..n_hot-1 are FP32 master rows updated by addition;
  * rows n_hot.. are BF16 bit patterns, read as FP32 and written back as
  * SR(value + update): 16 random bits added below the BF16 mantissa, then
- * truncation.  The bits of one (pair, slot, lane) come from a keyed stream:
- *   key    = H(seed ^ ((u32)s * 0x9E3779B1 + pair * 0x85EBCA77 + lane * 0xC2B2AE3D))
- *   stream = key + slot * 0x27D4EB2F
- *   word k = (stream = stream * 1664525 + 1013904223), one per two values:
- *            its low 16 bits round the lane's value 2k, its high 16 bits
- *            value 2k + 1
+ * truncation.  The bits of one (pair, slot, lane) come from the pair's key:
+ *   kp     = H(seed ^ ((u32)s * 0x9E3779B1 + pair * 0x85EBCA77))
+ *   x      = kp ^ (lane * 0xC2B2AE3D)
+ *   word k = (x + slot * 0x27D4EB2F + k * 0x165667B1) * 0x9E3779B1 (mod 2^32),
+ *            one per two values: its low 16 bits round the lane's value 2k,
+ *            its high 16 bits value 2k + 1
  * (s: sentence index in the plan; pair: index of the (center, context) pair in
  * the sentence, or of the center for CBOW)  * where H is a multiply / xor-shift mixer, slot = d (target index, 0 is the
  * positive) for syn1 rows and 256 (+ window position a for CBOW) for syn0
@@ -576,7 +576,7 @@ static uint32_t sr_h(uint32_t x) {
   return x;
 }
 uint32_t orc_lane_key(uint32_t seed, uint64_t s, uint32_t pair, uint32_t lane) {
-  return sr_h(seed ^ ((uint32_t)s * 0x9E3779B1u + pair * 0x85EBCA77u + lane * 0xC2B2AE3Du));
+  return sr_h(seed ^ ((uint32_t)s * 0x9E3779B1u + pair * 0x85EBCA77u)) ^ (lane * 0xC2B2AE3Du);
 }
 static float bf_to_f(uint16_t h) {
   uint32_t b = (uint32_t)h << 16;
@@ -613,13 +613,11 @@ static void mr_add(const mixed_rows *m, long long row, const float *cur, const f
   }
   uint16_t *b = m->bf + (row - m->n_hot) * m->dim;
   for (int lane = 0; lane < 32; lane++) {
-    uint32_t st = orc_lane_key(seed, s, pair, (uint32_t)lane) + slot * 0x27D4EB2Fu, w = 0;
+    const uint32_t x = orc_lane_key(seed, s, pair, (uint32_t)lane);
+    uint32_t w = 0;
     for (int j = 0; lane + 32 * j < m->dim; j++) {
       int t = lane + 32 * j;
-      if ((j & 1) == 0) {
-        st = st * 1664525u + 1013904223u;
-        w = st;
-      }
+      if ((j & 1) == 0) w = (x + slot * 0x27D4EB2Fu + (uint32_t)(j / 2) * 0x165667B1u) * 0x9E3779B1u;
       b[t] = f_to_bf_sr(cur[t] + u[t], (j & 1) ? (w >> 16) : (w & 0xFFFFu));
     }
   }

@@ -136,6 +136,7 @@ void orc_negreuse_batch(float *syn0, float *syn1, const float *exp_table, const 
  * 0..n_hot-1, stochastically rounded BF16 rows after them; rule in
  * felog_oracle.c).  syn*_bf hold (vocab_size - n_hot) * dim BF16 bit patterns,
  * logical dimension order. */
+/* the lane's mixed rounding key of (seed, sentence, pair) */
 uint32_t orc_lane_key(uint32_t seed, uint64_t s, uint32_t pair, uint32_t lane);
 uint32_t orc_round_sr_seed(uint64_t seed, uint32_t round);
 void orc_skipgram_bf16(float *syn0, uint16_t *syn0_bf, float *syn1, uint16_t *syn1_bf, long long n_hot,

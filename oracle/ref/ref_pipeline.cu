@@ -13,10 +13,18 @@
  * Rounds are not cut short (pauseWalk is never raised), so every round walks
  * all walkers - the same work the B200 path does per round.
  *
- * Usage: ref_pipeline graph.bin V warmup_rounds timed_rounds walkers
+ * Usage: ref_pipeline graph.bin V warmup_rounds timed_rounds walkers [emb_out]
  * Prints one JSON line: tokens, seconds (timed rounds, walk overlapped with
  * training as in the reference), walk_tokens, walk_seconds, train_words,
  * train_seconds, threads, walkers.
+ *
+ * emb_out (optional): after the last round, the trained tables in the
+ * reference's own -binary 1 layout (the writer of TrainModel,
+ * word2vec.cu:2119-2126: "<vocab_size> <layer1_size>\n", then per vocabulary
+ * row its word, a space, layer1_size raw floats and "\n") - syn0 as the
+ * trainer copied it back (word2vec.cu:1264), followed by the same rows of the
+ * device syn1neg table (d_syn1) so that the syn0 . syn1 link score can be
+ * formed too.
  */
 #include <cuda_runtime.h>
 
@@ -45,6 +53,7 @@ int main(int argc, char **argv) {
   uint32_t V = (uint32_t)strtoul(argv[2], nullptr, 10);
   int warm = atoi(argv[3]), timed = atoi(argv[4]);
   uint32_t walkers = (uint32_t)strtoul(argv[5], nullptr, 10);
+  const char *emb_out = argc > 6 ? argv[6] : nullptr;
   if (walkers == 0 || walkers > V) walkers = V;
   int total_rounds = warm + timed;
   int margc = 1;
@@ -161,6 +170,25 @@ int main(int argc, char **argv) {
   }
   trainer.join();
   graph.out_queue.closeQueue();
+  if (emb_out) {
+    std::vector<float> s1((size_t)vocab_size * layer1_size);
+    cudaMemcpy(s1.data(), d_syn1, s1.size() * sizeof(float), cudaMemcpyDeviceToHost);
+    FILE *fo = fopen(emb_out, "wb");
+    if (!fo) {
+      fprintf(stderr, "cannot open %s\n", emb_out);
+      return 1;
+    }
+    for (int t = 0; t < 2; t++) {
+      const float *tab = t == 0 ? syn0 : s1.data();
+      fprintf(fo, "%lld %lld\n", vocab_size, layer1_size);
+      for (long long a = 0; a < vocab_size; a++) {
+        fprintf(fo, "%s ", vocab[a].word);
+        fwrite(&tab[a * layer1_size], sizeof(float), layer1_size, fo);
+        fprintf(fo, "\n");
+      }
+    }
+    fclose(fo);
+  }
   printf("{\"tokens\": %llu, \"seconds\": %.6f, \"walk_tokens\": %llu, \"walk_seconds\": %.6f, "
          "\"train_words\": %llu, \"train_seconds\": %.6f, \"threads\": %d, \"walkers\": %u}\n",
          (unsigned long long)tokens, t_end - t_start, (unsigned long long)walk_tokens, walk_s > 0 ? walk_s : 1e-9,
