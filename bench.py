@@ -252,23 +252,32 @@ def new_context(fb, g, form, device, seed, model, autotune=1):
     return f
 
 
-def link_auc(f, g):
-    """Exact AUC of the held-out edges against the sampled non-edges, scored by
-    the cosine of the two endpoints' syn0 rows (FP64 on the host)."""
-    import felog_b200 as fb
-    s0, _ = f.embeddings()
-    _, id2, vs, _ = f.vocab()
-    e0 = s0.reshape(vs, -1)[id2]
-    del s0
-    def score(e):
-        e = e / np.maximum(np.linalg.norm(e, axis=1, keepdims=True), 1e-30)
-        cos = np.einsum("ij,ij->i", e[g["test_src"]], e[g["test_dst"]])
-        return float(fb.auc(cos.astype(np.float64), g["test_label"]))
-    raw = score(e0)
-    # the same cosine after removing the mean row (the direction that rarely
-    # trained rows share), for information
-    centered = score(e0 - e0.mean(axis=0, keepdims=True))
-    return raw, centered
+def quality(f, g, pairs):
+    """Link scores of the context's embedding (tests/ref_tables.py, FP64):
+    held-out AUC (held-out edges against the split's uniform non-edges, raw and
+    mean-centred cosine) and fit AUC (training edges against degree-matched
+    non-edges, mean-centred cosine and the skip-gram score)."""
+    import ref_tables as rt
+    s0, s1 = rt.tables_by_vertex(f)
+    held = rt.link_aucs(s0, s1, g)
+    fit = rt.fit_aucs(s0, s1, pairs)
+    return {"auc": held["cosine"], "auc_centered": held["cosine_centered"],
+            "fit_auc": fit["cosine_centered"], "fit_auc_sgns": fit["sgns"]}
+
+
+def reference_quality(g, pairs):
+    """The same scores of the reference's own run (oracle/_ref/ref_pipeline:
+    its walk engine and CUDA skip_gram_kernel) after the same two rounds."""
+    import ref_tables as rt
+    if not os.path.exists(rt.REF_PIPELINE):
+        return {"unavailable": "oracle/_ref/ref_pipeline was not built"}
+    t0 = time.perf_counter()
+    s0, s1 = rt.run_reference(g["edges"], g["v_num"], TRAIN["min_rounds"])
+    held = rt.link_aucs(s0, s1, g)
+    fit = rt.fit_aucs(s0, s1, pairs)
+    return {"rounds": TRAIN["min_rounds"], "auc": held["cosine"], "auc_centered": held["cosine_centered"],
+            "fit_auc": fit["cosine_centered"], "fit_auc_sgns": fit["sgns"],
+            "wall_s": time.perf_counter() - t0}
 
 
 def compare_forms(fb, g, device, model):
@@ -276,6 +285,9 @@ def compare_forms(fb, g, device, model):
     train and budget check until the stop-all rule) on the same graph and walk
     seed; job time is the device time of the second of two runs in one context
     (the first one pays for allocations)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import ref_tables as rt
+    pairs = rt.fit_pairs(g)
     out = {}
     for form in ("plain-fp32", "learned-bf16", "learned-bf16-tile", "learned-fp32-tile"):
         f = new_context(fb, g, form, device, 77, model)
@@ -288,13 +300,20 @@ def compare_forms(fb, g, device, model):
                      "job_ms": rs["total_ms"], "wall_ms": wall * 1e3,
                      "tokens_per_s": rs["walk_tokens"] / (rs["total_ms"] * 1e-3),
                      "budget": {k: rs[k] for k in ("evaluated", "predicted", "audited", "overruled")}}
-        out[form]["auc"], out[form]["auc_centered"] = link_auc(f, g)
+        out[form].update(quality(f, g, pairs))
         f.close()
     p = out["plain-fp32"]
     for form in ("learned-bf16", "learned-bf16-tile", "learned-fp32-tile"):
         out[form]["end_to_end_speedup_vs_plain_fp32"] = p["job_ms"] / out[form]["job_ms"]
-        out[form]["auc_delta_vs_plain_fp32"] = out[form]["auc"] - p["auc"]
-        out[form]["auc_centered_delta_vs_plain_fp32"] = out[form]["auc_centered"] - p["auc_centered"]
+        for k in ("auc", "auc_centered", "fit_auc", "fit_auc_sgns"):
+            out[form][k + "_delta_vs_plain_fp32"] = out[form][k] - p[k]
+    out["reference"] = reference_quality(g, pairs)
+    if "fit_auc" in out["reference"]:
+        for k in ("auc", "fit_auc", "fit_auc_sgns"):
+            p[k + "_delta_vs_reference"] = p[k] - out["reference"][k]
+    out["scores"] = ("auc: held-out edges vs the split's uniform non-edges, raw cosine; fit_auc: training edges vs "
+                     "degree-matched non-edges, mean-centred cosine (the score the 0.005 bar applies to); "
+                     "fit_auc_sgns: the same pairs by syn0[u].syn1[v] (symmetrised)")
     return out
 
 

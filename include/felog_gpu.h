@@ -27,6 +27,8 @@
  *                           train_corpus_cuda, src/examples/felog.cpp:33-172,
  *                           src/word2vec.cu:1922-2180
  *   felog_write_embeddings  the -emb_output writer, src/word2vec.cu:2112-2127
+ *   felog_load_rmat         the synthetic stand-ins of the reference's datasets
+ *                           (no reference counterpart), generated on the device
  */
 #ifndef FELOG_GPU_H
 #define FELOG_GPU_H
@@ -38,7 +40,7 @@
 extern "C" {
 #endif
 
-#define FELOG_ABI_VERSION 2
+#define FELOG_ABI_VERSION 3
 
 typedef enum felog_status {
   FELOG_OK = 0,
@@ -103,6 +105,8 @@ typedef struct felog_opts {
   float budget_confidence;  /* learned budget: predictions below this softmax confidence fall back (0: 0.9) */
   float budget_audit;       /* learned budget: fraction of confident vertices re-checked (0: 0.05; <0: none) */
   int32_t autotune;         /* 1 (default): the first round picks the pair trainer's launch shape by timing */
+  uint32_t stream_walkers;  /* felog_run: walk and train each round in pieces of this many walkers, so the
+                               corpus of a whole round is never resident (0: whole rounds) */
 } felog_opts;
 
 typedef struct felog_ctx felog_ctx;
@@ -178,11 +182,41 @@ int felog_abi_version(void);
 /* ---- graph ---- */
 /* n records of the 12-byte binary format; doubled (e, e^T interleaved) when
  * undirected; CSR bucketed by source in record order (graph.hpp:531-575).
- * Limits: at most 2^31-1 CSR entries and 2^31-2 vertices (FELOG_INVALID_ARG
- * beyond; the build sorts and scans with 32-bit counts). */
+ * Limits: at most 2^32-1 CSR entries (32-bit entry indices; the sorts and
+ * scans count in 64 bits) and 2^31-2 vertices (FELOG_INVALID_ARG beyond).
+ * Building the CSR of m entries holds 12 n + 24 m bytes of device scratch. */
 felog_status felog_load_graph(felog_ctx *ctx, const felog_edge12 *edges, uint64_t n, uint32_t v_num,
                               int undirected);
 felog_status felog_load_graph_file(felog_ctx *ctx, const char *path, uint32_t v_num, int undirected);
+
+/* No counterpart in the reference (its datasets are files; this builds the
+ * seeded R-MAT stand-ins on the device, at sizes a host edge list cannot
+ * carry).  The graph equals felog_synth_generate (include/felog_tools.h) with
+ * holdout 0 followed by felog_load_graph of its edges: the first e_target
+ * distinct unordered pairs of the counter-based R-MAT candidate stream,
+ * optionally permuted, untouched vertices dropped and the rest renumbered,
+ * weights uniform in (0, 1] or lognormal (lognormal weights use the device's
+ * FP64 log/cos/exp, so a weight may differ from the host's in its last bit).
+ * Candidates are drawn (2 e_target at first, up to 2^32) until e_target
+ * distinct pairs exist, else the graph keeps the pairs found.  Peak device
+ * memory about 24 bytes per candidate, then the CSR build of felog_load_graph.
+ * Needs v_target <= 2^31-2 and at most 2^32-1 CSR entries. */
+typedef struct felog_rmat_params {
+  uint64_t seed;
+  uint64_t v_target;       /* vertex ids drawn from [0, v_target) */
+  uint64_t e_target;       /* distinct undirected edges wanted */
+  double a, b, c, d;       /* quadrant probabilities */
+  int32_t lognormal;       /* 0: weights uniform in (0, 1]; 1: lognormal(mu, sigma) */
+  double lognormal_mu, lognormal_sigma;
+  int32_t permute_ids;     /* 1: relabel vertex ids by the seeded permutation */
+} felog_rmat_params;
+typedef struct felog_rmat_info {
+  uint32_t v_num;          /* vertices kept (ids 0 .. v_num - 1) */
+  uint64_t n_edges;        /* undirected edges (records) */
+  uint32_t max_degree;
+} felog_rmat_info;
+felog_status felog_load_rmat(felog_ctx *ctx, const felog_rmat_params *params, int undirected,
+                             felog_rmat_info *info);
 felog_status felog_graph_info(felog_ctx *ctx, uint32_t *v_num, uint64_t *e_num);
 felog_status felog_get_csr(felog_ctx *ctx, uint64_t *row_ptr, uint32_t *nbr, float *data);
 felog_status felog_get_degrees(felog_ctx *ctx, uint32_t *deg);
@@ -220,6 +254,17 @@ felog_status felog_get_stop_flags(felog_ctx *ctx, uint8_t *flags);
 /* round: 0-based round index (part of the Philox counter). draws: NULL for the
  * native Philox stream. */
 felog_status felog_walk_round(felog_ctx *ctx, uint32_t round, const felog_draws *draws,
+                              felog_walk_stats *stats);
+/* One piece of a round (no reference counterpart; the reference holds a whole
+ * round's corpus): the active walkers first .. first + count - 1 of round
+ * `round` walk, and their walks become the corpus, so a caller can train
+ * piece by piece and never hold a round's corpus (a 111M-vertex round is
+ * about 2.4 G tokens).  first == 0 rebuilds the round's active walker list
+ * from the stop flags; *n_active (optional) returns its length.  The walks
+ * are those felog_walk_round makes (Philox draws keyed by walker); the
+ * round KL is computed with the last piece.  The next felog_train_round
+ * trains on the piece with its own rounding seed. */
+felog_status felog_walk_piece(felog_ctx *ctx, uint32_t round, uint64_t first, uint64_t count, uint64_t *n_active,
                               felog_walk_stats *stats);
 felog_status felog_corpus_size(felog_ctx *ctx, uint64_t *n_sentences, uint64_t *n_tokens);
 /* sentences in walker-id order; sent_off: n_sentences + 1 entries */

@@ -26,6 +26,7 @@
 #include "mlp.cuh"
 #include "pairs.cuh"
 #include "plan.cuh"
+#include "rmat.cuh"
 #include "sgns.cuh"
 #include "walk.cuh"
 
@@ -34,6 +35,10 @@ using namespace felog;
 namespace {
 
 constexpr int64_t kTableSize = 100000000;  // table_size, word2vec.cu:171
+// Vocabularies up to this size use the reference's table; larger ones a
+// table of 8 slots per word (the reference's 1e8 slots would leave most of a
+// 111M-word vocabulary without one).
+constexpr long long kRefTableMaxVocab = kTableSize / 8;
 constexpr uint64_t kPairChunk = 1ull << 27;  // pair records generated and trained per chunk
 
 template <class T>
@@ -95,6 +100,7 @@ struct felog_ctx {
   DevBuf<uint8_t> stop;
   DevBuf<uint32_t> active;
   uint32_t n_active = 0;
+  uint32_t chunk_base = 0;  // first active walker of the corpus (streamed rounds; 0 otherwise)
   DevBuf<uint32_t> arena;
   uint64_t arena_cap = 0;
   uint64_t spill_base = 0;
@@ -128,6 +134,7 @@ struct felog_ctx {
   DevBuf<uint16_t> thr;
   bool use_thr = false;
   DevBuf<int32_t> table;
+  uint64_t table_size = kTableSize;  // unigram slots (more for vocabularies beyond kRefTableMaxVocab)
   DevBuf<uint32_t> table_coarse;  // per 64-slot bucket: first word, top bit when uniform
   DevBuf<float> exp_table;
   DevBuf<float> syn0, syn1;        // FP32 rows 0..n_f32-1 (all rows in FP32 mode)
@@ -398,25 +405,14 @@ extern "C" const char *felog_last_error(const felog_ctx *c) { return c ? c->err.
 
 // ----------------------------------------------------------------- graph
 
-extern "C" felog_status felog_load_graph(felog_ctx *c, const felog_edge12 *edges, uint64_t n, uint32_t v_num,
-                                         int undirected) {
-  if (!c) return FELOG_INVALID_ARG;
-  if (v_num == 0) return fail(c, FELOG_INVALID_ARG, "load_graph: v_num must be > 0");
-  if (n && !edges) return fail(c, FELOG_INVALID_ARG, "load_graph: edges is NULL");
-  uint64_t m = undirected ? 2 * n : n;
-  // the CSR build sorts and scans with 32-bit signed counts
-  if (m > 0x7FFFFFFFULL) return fail(c, FELOG_INVALID_ARG, "load_graph: more than 2^31-1 CSR entries");
-  if (v_num > 0x7FFFFFFEu) return fail(c, FELOG_INVALID_ARG, "load_graph: more than 2^31-2 vertices");
-  // the previous graph is gone as soon as its buffers are reused
-  c->V = 0;
-  c->M = 0;
-  c->model_ready = false;
-  c->corpus_ready = false;
-  c->has_alias = false;
-  CK(cudaSetDevice(c->device), "load_graph");
-  DevBuf<uint32_t> rec, keys, vals, keys2, vals2;
-  CK(rec.ensure(3 * std::max<uint64_t>(n, 1)), "load_graph: records");
-  if (n) CK(cudaMemcpyAsync(rec.p, edges, n * 12, cudaMemcpyHostToDevice, c->stream), "load_graph: upload");
+namespace {
+
+// CSR of n device records (3 words each: src, dst, data bits), doubled when
+// undirected; the records stay the caller's.  Entry indices are 32-bit, so at
+// most 2^32 - 1 directed entries; the sorts and scans count items in 64 bits.
+felog_status build_csr(felog_ctx *c, const uint32_t *rec, uint64_t n, uint32_t v_num, int undirected) {
+  const uint64_t m = undirected ? 2 * n : n;
+  DevBuf<uint32_t> keys, vals, keys2, vals2;
   CK(keys.ensure(m), "load_graph");
   CK(vals.ensure(m), "load_graph");
   CK(keys2.ensure(m), "load_graph");
@@ -427,19 +423,19 @@ extern "C" felog_status felog_load_graph(felog_ctx *c, const felog_edge12 *edges
   CK(cudaMemsetAsync(c->deg.p, 0, sizeof(uint32_t) * v_num, c->stream), "load_graph");
   CK(cudaMemsetAsync(c->derr.p, 0, sizeof(int), c->stream), "load_graph");
   if (m) {
-    k_expand_edges<<<grid_for(c, m, 256), 256, 0, c->stream>>>(rec.p, n, undirected, v_num, keys.p, vals.p,
-                                                                  c->deg.p, c->derr.p);
+    k_expand_edges<<<grid_for(c, m, 256), 256, 0, c->stream>>>(rec, n, undirected, v_num, keys.p, vals.p, c->deg.p,
+                                                                  c->derr.p);
     c->launches++;
     CK(cudaGetLastError(), "load_graph: expand");
     int end_bit = 1;
     while (end_bit < 32 && (1ULL << end_bit) < v_num) end_bit++;
     cub::DoubleBuffer<uint32_t> dk(keys.p, keys2.p), dv(vals.p, vals2.p);
     size_t tmp = 0;
-    CK(cub::DeviceRadixSort::SortPairs(nullptr, tmp, dk, dv, (int)m, 0, end_bit, c->stream), "load_graph: sort");
+    CK(cub::DeviceRadixSort::SortPairs(nullptr, tmp, dk, dv, (int64_t)m, 0, end_bit, c->stream), "load_graph: sort");
     CK(c->cub_tmp.ensure(tmp), "load_graph: sort scratch");
-    CK(cub::DeviceRadixSort::SortPairs(c->cub_tmp.p, tmp, dk, dv, (int)m, 0, end_bit, c->stream),
+    CK(cub::DeviceRadixSort::SortPairs(c->cub_tmp.p, tmp, dk, dv, (int64_t)m, 0, end_bit, c->stream),
        "load_graph: sort");
-    k_gather_adj<<<grid_for(c, m, 256), 256, 0, c->stream>>>(rec.p, dv.Current(), m, undirected, c->adj.p);
+    k_gather_adj<<<grid_for(c, m, 256), 256, 0, c->stream>>>(rec, dv.Current(), m, undirected, c->adj.p);
     c->launches++;
     CK(cudaGetLastError(), "load_graph: gather");
   }
@@ -447,10 +443,10 @@ extern "C" felog_status felog_load_graph(felog_ctx *c, const felog_edge12 *edges
   {
     CK(cudaMemsetAsync(c->row_ptr.p, 0, sizeof(uint64_t), c->stream), "load_graph");
     size_t tmp = 0;
-    CK(cub::DeviceScan::InclusiveSum(nullptr, tmp, c->deg.p, c->row_ptr.p + 1, (int)v_num, c->stream),
+    CK(cub::DeviceScan::InclusiveSum(nullptr, tmp, c->deg.p, c->row_ptr.p + 1, (int64_t)v_num, c->stream),
        "load_graph: scan");
     CK(c->cub_tmp.ensure(tmp), "load_graph: scan scratch");
-    CK(cub::DeviceScan::InclusiveSum(c->cub_tmp.p, tmp, c->deg.p, c->row_ptr.p + 1, (int)v_num, c->stream),
+    CK(cub::DeviceScan::InclusiveSum(c->cub_tmp.p, tmp, c->deg.p, c->row_ptr.p + 1, (int64_t)v_num, c->stream),
        "load_graph: scan");
   }
   felog_status s = check_dev_err(c, "load_graph");
@@ -459,7 +455,8 @@ extern "C" felog_status felog_load_graph(felog_ctx *c, const felog_edge12 *edges
   CK(cudaMemcpyAsync(c->h_deg.data(), c->deg.p, sizeof(uint32_t) * v_num, cudaMemcpyDeviceToHost, c->stream),
      "load_graph");
   CK(cudaStreamSynchronize(c->stream), "load_graph");
-  rec.release(); keys.release(); vals.release(); keys2.release(); vals2.release();
+  keys.release(); vals.release(); keys2.release(); vals2.release();
+  c->cub_tmp.release();
   c->V = v_num;
   c->M = m;
   c->has_alias = false;
@@ -472,6 +469,174 @@ extern "C" felog_status felog_load_graph(felog_ctx *c, const felog_edge12 *edges
   CK(c->visit_freq.ensure(v_num), "load_graph");
   CK(cudaMemsetAsync(c->visit_freq.p, 0, sizeof(unsigned int) * v_num, c->stream), "load_graph");
   CK(cudaStreamSynchronize(c->stream), "load_graph");
+  return FELOG_OK;
+}
+
+// the previous graph is gone as soon as its buffers are reused
+void forget_graph(felog_ctx *c) {
+  c->V = 0;
+  c->M = 0;
+  c->model_ready = false;
+  c->corpus_ready = false;
+  c->has_alias = false;
+}
+
+}  // namespace
+
+extern "C" felog_status felog_load_graph(felog_ctx *c, const felog_edge12 *edges, uint64_t n, uint32_t v_num,
+                                         int undirected) {
+  if (!c) return FELOG_INVALID_ARG;
+  if (v_num == 0) return fail(c, FELOG_INVALID_ARG, "load_graph: v_num must be > 0");
+  if (n && !edges) return fail(c, FELOG_INVALID_ARG, "load_graph: edges is NULL");
+  const uint64_t m = undirected ? 2 * n : n;
+  // 32-bit entry indices (the sorts count items in 64 bits)
+  if (m > 0xFFFFFFFFULL) return fail(c, FELOG_INVALID_ARG, "load_graph: more than 2^32-1 CSR entries");
+  if (v_num > 0x7FFFFFFEu) return fail(c, FELOG_INVALID_ARG, "load_graph: more than 2^31-2 vertices");
+  forget_graph(c);
+  CK(cudaSetDevice(c->device), "load_graph");
+  DevBuf<uint32_t> rec;
+  CK(rec.ensure(3 * std::max<uint64_t>(n, 1)), "load_graph: records");
+  if (n) CK(cudaMemcpyAsync(rec.p, edges, n * 12, cudaMemcpyHostToDevice, c->stream), "load_graph: upload");
+  return build_csr(c, rec.p, n, v_num, undirected);
+}
+
+extern "C" felog_status felog_load_rmat(felog_ctx *c, const felog_rmat_params *p, int undirected,
+                                        felog_rmat_info *info) {
+  if (!c || !p) return FELOG_INVALID_ARG;
+  const double sum = p->a + p->b + p->c + p->d;
+  if (p->v_target < 2 || p->v_target > 0x7FFFFFFEull || p->e_target == 0 || !(sum > 0.999 && sum < 1.001))
+    return fail(c, FELOG_INVALID_ARG, "load_rmat: need 2 <= v_target <= 2^31-2, e_target > 0, a+b+c+d = 1");
+  if ((undirected ? 2 : 1) * p->e_target > 0xFFFFFFFFull)
+    return fail(c, FELOG_INVALID_ARG, "load_rmat: more than 2^32-1 CSR entries");
+  forget_graph(c);
+  CK(cudaSetDevice(c->device), "load_rmat");
+  RmatArgs a{};
+  a.hs = rmat_mix64(p->seed ^ 0x5DEECE66DULL);
+  a.hw = rmat_mix64((p->seed ^ 0x77ULL) ^ 0x5DEECE66DULL);
+  a.V = p->v_target;
+  while ((1ULL << a.scale) < a.V) a.scale++;
+  a.ta = p->a;
+  a.tab = p->a + p->b;
+  a.tabc = p->a + p->b + p->c;
+  a.lognormal = p->lognormal;
+  a.mu = p->lognormal_mu;
+  a.sigma = p->lognormal_sigma;
+  // candidates until e_target distinct pairs are among them (each try starts
+  // over with more; the first e_target pairs in candidate order do not depend
+  // on how many candidates were drawn beyond them)
+  DevBuf<uint32_t> kept;
+  uint64_t E = 0;
+  for (uint64_t n = std::min<uint64_t>(2 * p->e_target + 1024, 0xFFFFFFFFull);;) {
+    DevBuf<uint64_t> key, key2;
+    DevBuf<uint32_t> idx, idx2;
+    DevBuf<uint8_t> flag;
+    DevBuf<unsigned long long> cnt;
+    CK(key.ensure(n), "load_rmat: candidates");
+    CK(key2.ensure(n), "load_rmat: candidates");
+    CK(idx.ensure(n), "load_rmat: candidates");
+    CK(idx2.ensure(n), "load_rmat: candidates");
+    CK(cnt.ensure(1), "load_rmat");
+    k_rmat_candidates<<<grid_for(c, n, 256), 256, 0, c->stream>>>(a, 0, n, key.p, idx.p);
+    c->launches++;
+    CK(cudaGetLastError(), "load_rmat: candidates");
+    cub::DoubleBuffer<uint64_t> dk(key.p, key2.p);
+    cub::DoubleBuffer<uint32_t> dv(idx.p, idx2.p);
+    size_t tmp = 0;
+    const int end_bit = std::min(64, 32 + a.scale);
+    CK(cub::DeviceRadixSort::SortPairs(nullptr, tmp, dk, dv, (int64_t)n, 0, end_bit, c->stream), "load_rmat: sort");
+    CK(c->cub_tmp.ensure(tmp), "load_rmat: sort scratch");
+    CK(cub::DeviceRadixSort::SortPairs(c->cub_tmp.p, tmp, dk, dv, (int64_t)n, 0, end_bit, c->stream),
+       "load_rmat: sort");
+    CK(flag.ensure(n), "load_rmat: flags");
+    k_rmat_first<<<grid_for(c, n, 256), 256, 0, c->stream>>>(dk.Current(), n, flag.p);
+    c->launches++;
+    uint32_t *firsts = dk.Current() == key.p ? reinterpret_cast<uint32_t *>(key2.p) : reinterpret_cast<uint32_t *>(key.p);
+    tmp = 0;
+    CK(cub::DeviceSelect::Flagged(nullptr, tmp, dv.Current(), flag.p, firsts, cnt.p, (int64_t)n, c->stream),
+       "load_rmat: select");
+    CK(c->cub_tmp.ensure(tmp), "load_rmat: select scratch");
+    CK(cub::DeviceSelect::Flagged(c->cub_tmp.p, tmp, dv.Current(), flag.p, firsts, cnt.p, (int64_t)n, c->stream),
+       "load_rmat: select");
+    unsigned long long U = 0;
+    RB(&U, cnt.p, sizeof U, "load_rmat");
+    if (U < p->e_target && n < 0xFFFFFFFFull) {
+      n = std::min<uint64_t>(n + n / 2, 0xFFFFFFFFull);
+      continue;
+    }
+    // the distinct pairs' first candidates in candidate order, cut at e_target
+    uint32_t *sorted = dv.Current() == idx.p ? idx2.p : idx.p;
+    cub::DoubleBuffer<uint32_t> dd(firsts, sorted);
+    int ib = 1;
+    while (ib < 32 && (1ULL << ib) < n) ib++;
+    tmp = 0;
+    CK(cub::DeviceRadixSort::SortKeys(nullptr, tmp, dd, (int64_t)U, 0, ib, c->stream), "load_rmat: order");
+    CK(c->cub_tmp.ensure(tmp), "load_rmat: order scratch");
+    CK(cub::DeviceRadixSort::SortKeys(c->cub_tmp.p, tmp, dd, (int64_t)U, 0, ib, c->stream), "load_rmat: order");
+    E = std::min<uint64_t>(U, p->e_target);
+    CK(kept.ensure(std::max<uint64_t>(E, 1)), "load_rmat");
+    CK(cudaMemcpyAsync(kept.p, dd.Current(), 4 * E, cudaMemcpyDeviceToDevice, c->stream), "load_rmat");
+    CK(cudaStreamSynchronize(c->stream), "load_rmat");
+    break;
+  }
+  c->cub_tmp.release();
+  const uint64_t V = p->v_target;
+  // optional relabelling: the host generator's Fisher-Yates (sequential, on the host)
+  DevBuf<uint32_t> perm;
+  if (p->permute_ids) {
+    std::vector<uint32_t> hp(V);
+    for (uint64_t i = 0; i < V; i++) hp[i] = (uint32_t)i;
+    const uint64_t hf = rmat_mix64((p->seed ^ 0xA5A5A5A5ULL) ^ 0x5DEECE66DULL);
+    for (uint64_t i = V - 1; i > 0; i--) std::swap(hp[i], hp[rmat_draw(hf, 0xFFFFFFFFULL, i) % (i + 1)]);
+    CK(perm.ensure(V), "load_rmat");
+    CK(cudaMemcpy(perm.p, hp.data(), 4 * V, cudaMemcpyHostToDevice), "load_rmat");
+  }
+  // drop untouched vertices, renumber the rest in increasing order
+  DevBuf<uint8_t> touched;
+  DevBuf<uint32_t> t32, newid;
+  CK(touched.ensure(V), "load_rmat");
+  CK(cudaMemsetAsync(touched.p, 0, V, c->stream), "load_rmat");
+  if (E) {
+    k_rmat_touch<<<grid_for(c, E, 256), 256, 0, c->stream>>>(a, kept.p, E, perm.p, touched.p);
+    c->launches++;
+  }
+  CK(t32.ensure(V + 1), "load_rmat");
+  CK(newid.ensure(V + 1), "load_rmat");
+  CK(cudaMemsetAsync(t32.p + V, 0, 4, c->stream), "load_rmat");
+  k_u8_to_u32<<<grid_for(c, V, 256), 256, 0, c->stream>>>(touched.p, V, t32.p);
+  c->launches++;
+  size_t tmp = 0;
+  CK(cub::DeviceScan::ExclusiveSum(nullptr, tmp, t32.p, newid.p, (int64_t)(V + 1), c->stream), "load_rmat: scan");
+  CK(c->cub_tmp.ensure(tmp), "load_rmat: scan scratch");
+  CK(cub::DeviceScan::ExclusiveSum(c->cub_tmp.p, tmp, t32.p, newid.p, (int64_t)(V + 1), c->stream),
+     "load_rmat: scan");
+  uint32_t nv = 0;
+  RB(&nv, newid.p + V, 4, "load_rmat");
+  touched.release();
+  t32.release();
+  if (nv == 0) return fail(c, FELOG_INVALID_ARG, "load_rmat: no edges drawn");
+  DevBuf<uint32_t> rec;
+  CK(rec.ensure(3 * std::max<uint64_t>(E, 1)), "load_rmat: records");
+  if (E) {
+    k_rmat_records<<<grid_for(c, E, 256), 256, 0, c->stream>>>(a, kept.p, E, perm.p, newid.p, rec.p);
+    c->launches++;
+    CK(cudaGetLastError(), "load_rmat: records");
+  }
+  kept.release();
+  perm.release();
+  newid.release();
+  felog_status s = build_csr(c, rec.p, E, nv, undirected);
+  if (s != FELOG_OK) return s;
+  if (info) {
+    memset(info, 0, sizeof(*info));
+    info->v_num = nv;
+    info->n_edges = E;
+    CK(cudaMemsetAsync(c->counters.p, 0, 8, c->stream), "load_rmat");
+    k_max_u32<<<grid_for(c, nv, 256), 256, 0, c->stream>>>(c->deg.p, nv, (unsigned int *)c->counters.p);
+    c->launches++;
+    unsigned int md = 0;
+    RB(&md, c->counters.p, 4, "load_rmat");
+    info->max_degree = md;
+  }
   return FELOG_OK;
 }
 
@@ -650,17 +815,15 @@ felog_status round_kl(felog_ctx *c, double *out) {
 
 }  // namespace
 
-extern "C" felog_status felog_walk_round(felog_ctx *c, uint32_t round, const felog_draws *draws,
-                                         felog_walk_stats *stats) {
-  if (!c) return FELOG_INVALID_ARG;
-  if (!c->V) return fail(c, FELOG_NOT_READY, "no graph loaded");
-  if (c->o.weighted && !c->has_alias) return fail(c, FELOG_NOT_READY, "weighted walk needs felog_build_alias");
-  CK(cudaSetDevice(c->device), "walk_round");
-  const uint32_t walker_num = c->o.walker_num ? c->o.walker_num : c->V;
-  if (walker_num > 0x7FFFFFFEu) return fail(c, FELOG_INVALID_ARG, "walk_round: more than 2^31-2 walkers");
-  felog_status s = build_active(c, walker_num);
-  if (s != FELOG_OK) return s;
-  const uint32_t na = c->n_active;
+namespace {
+
+// Walks the active walkers k0 .. k1 - 1 of the round (after build_active);
+// their walks become the corpus.  with_kl: also the round relative entropy
+// (after the last range of a round).
+felog_status walk_range(felog_ctx *c, uint32_t round, const felog_draws *draws, uint32_t k0, uint32_t k1,
+                        felog_walk_stats *stats, bool with_kl) {
+  felog_status s;
+  const uint32_t na = k1 - k0;
   if (draws && draws->n_walkers != na)
     return fail(c, FELOG_INVALID_ARG, "walk_round: draws cover %llu walkers, %u are active",
                 (unsigned long long)draws->n_walkers, na);
@@ -708,7 +871,7 @@ extern "C" felog_status felog_walk_round(felog_ctx *c, uint32_t round, const fel
   a.alias_idx = c->alias_idx.p;
   a.v_num = c->V;
   a.n_active = na;
-  a.active = c->active.p;
+  a.active = c->active.p + k0;
   a.min_len = c->o.min_length;
   a.round = round;
   a.seed = c->o.seed;
@@ -760,7 +923,7 @@ extern "C" felog_status felog_walk_round(felog_ctx *c, uint32_t round, const fel
   s = budget_records(c);
   if (s != FELOG_OK) return s;
   if (na) {
-    k_budget_record_walk<<<grid_for(c, na, 256), 256, 0, c->stream>>>(c->active.p, na, c->V, c->sent_len.p,
+    k_budget_record_walk<<<grid_for(c, na, 256), 256, 0, c->stream>>>(c->active.p + k0, na, c->V, c->sent_len.p,
                                                                      c->bud_walks.p, c->bud_len_sum.p,
                                                                      c->bud_first_len.p);
     c->launches++;
@@ -775,10 +938,52 @@ extern "C" felog_status felog_walk_round(felog_ctx *c, uint32_t round, const fel
     stats->n_iterations = h[2];
     stats->n_long = h[3];
     stats->ms = ms;
-    s = round_kl(c, &stats->kl);
-    if (s != FELOG_OK) return s;
+    stats->kl = NAN;
+    if (with_kl) {
+      s = round_kl(c, &stats->kl);
+      if (s != FELOG_OK) return s;
+    }
   }
   return FELOG_OK;
+}
+
+felog_status walk_prepare(felog_ctx *c) {
+  if (!c->V) return fail(c, FELOG_NOT_READY, "no graph loaded");
+  if (c->o.weighted && !c->has_alias) return fail(c, FELOG_NOT_READY, "weighted walk needs felog_build_alias");
+  CK(cudaSetDevice(c->device), "walk_round");
+  const uint32_t walker_num = c->o.walker_num ? c->o.walker_num : c->V;
+  if (walker_num > 0x7FFFFFFEu) return fail(c, FELOG_INVALID_ARG, "walk_round: more than 2^31-2 walkers");
+  return build_active(c, walker_num);
+}
+
+}  // namespace
+
+extern "C" felog_status felog_walk_piece(felog_ctx *c, uint32_t round, uint64_t first, uint64_t count,
+                                         uint64_t *n_active, felog_walk_stats *stats) {
+  if (!c) return FELOG_INVALID_ARG;
+  felog_status s;
+  if (first == 0) {
+    s = walk_prepare(c);
+    if (s != FELOG_OK) return s;
+  } else if (!c->V) {
+    return fail(c, FELOG_NOT_READY, "no graph loaded");
+  }
+  const uint64_t na = c->n_active;
+  if (n_active) *n_active = na;
+  if (first > na) return fail(c, FELOG_INVALID_ARG, "walk_piece: first walker %llu past the %llu active ones",
+                              (unsigned long long)first, (unsigned long long)na);
+  const uint64_t last = std::min<uint64_t>(na, first + count);
+  c->chunk_base = (uint32_t)first;
+  return walk_range(c, round, nullptr, (uint32_t)first, (uint32_t)last, stats, last == na);
+}
+
+extern "C" felog_status felog_walk_round(felog_ctx *c, uint32_t round, const felog_draws *draws,
+                                         felog_walk_stats *stats) {
+  if (!c) return FELOG_INVALID_ARG;
+  felog_status s = walk_prepare(c);
+  if (s != FELOG_OK) return s;
+  c->chunk_base = 0;
+  return walk_range(c, round, draws, 0, c->n_active, stats, true);
 }
 
 namespace {
@@ -989,6 +1194,7 @@ extern "C" felog_status felog_get_corpus(felog_ctx *c, uint32_t *tokens, uint64_
 
 extern "C" felog_status felog_set_corpus(felog_ctx *c, const uint32_t *tokens, const uint64_t *sent_off,
                                          uint64_t n_sentences) {
+  if (c) c->chunk_base = 0;
   if (!c || !sent_off || (n_sentences && !tokens)) return FELOG_INVALID_ARG;
   if (!c->V) return fail(c, FELOG_NOT_READY, "no graph loaded");
   uint64_t ntok = sent_off[n_sentences];
@@ -1064,6 +1270,39 @@ __global__ void k_init_syn0(float *syn0, uint16_t *syn0_bf, uint64_t n_f32, uint
 
 }  // namespace
 
+namespace {
+// vocabulary sort keys: ~degree (a stable ascending sort gives degree descending), vertex id
+__global__ void k_vocab_keys(const uint32_t *__restrict__ deg, uint32_t V, uint32_t *__restrict__ key,
+                             uint32_t *__restrict__ val) {
+  for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V; v += (uint64_t)gridDim.x * blockDim.x) {
+    key[v] = ~deg[v];
+    val[v] = (uint32_t)v;
+  }
+}
+// degree^0.75 per vocabulary row (rows by id2offset; words outside the vocabulary skipped)
+__global__ void k_unigram_weights(const uint32_t *__restrict__ deg, const uint32_t *__restrict__ id2offset,
+                                  uint32_t V, double *__restrict__ w) {
+  for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V; v += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t r = id2offset[v];
+    if (r != 0xFFFFFFFFu) w[r] = pow((double)deg[v], 0.75);
+  }
+}
+// slot a -> first row whose cumulative weight exceeds (a + 1/2) / T of the total
+__global__ void k_unigram_fill(const double *__restrict__ cum, uint64_t n, uint64_t T, int32_t *__restrict__ table) {
+  const double total = cum[n - 1];
+  for (uint64_t a = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; a < T; a += (uint64_t)gridDim.x * blockDim.x) {
+    const double x = ((double)a + 0.5) / (double)T * total;
+    uint64_t lo = 0, hi = n - 1;
+    while (lo < hi) {
+      const uint64_t mid = (lo + hi) >> 1;
+      if (cum[mid] > x) hi = mid;
+      else lo = mid + 1;
+    }
+    table[a] = (int32_t)lo;
+  }
+}
+}  // namespace
+
 extern "C" felog_status felog_init_model(felog_ctx *c) {
   if (!c) return FELOG_INVALID_ARG;
   if (!c->V) return fail(c, FELOG_NOT_READY, "no graph loaded");
@@ -1076,11 +1315,26 @@ extern "C" felog_status felog_init_model(felog_ctx *c) {
   if (c->o.precision != FELOG_FP32 && c->o.precision != FELOG_BF16)
     return fail(c, FELOG_INVALID_ARG, "precision %d: use FELOG_FP32 or FELOG_BF16", c->o.precision);
   CK(cudaSetDevice(c->device), "init_model");
-  // vocabulary from degrees: stable sort, degree descending (word2vec.cu:834-862, :734-755)
+  // vocabulary from degrees: stable sort, degree descending (word2vec.cu:834-862, :734-755),
+  // as a stable radix sort of (~degree, vertex) on the device
   const uint32_t V = c->V;
   std::vector<uint32_t> order(V);
-  std::iota(order.begin(), order.end(), 0u);
-  std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return c->h_deg[a] > c->h_deg[b]; });
+  {
+    DevBuf<uint32_t> k0, k1, v0, v1;
+    CK(k0.ensure(V), "init_model: vocabulary");
+    CK(k1.ensure(V), "init_model: vocabulary");
+    CK(v0.ensure(V), "init_model: vocabulary");
+    CK(v1.ensure(V), "init_model: vocabulary");
+    k_vocab_keys<<<grid_for(c, V, 256), 256, 0, c->stream>>>(c->deg.p, V, k0.p, v0.p);
+    c->launches++;
+    cub::DoubleBuffer<uint32_t> dk(k0.p, k1.p), dv(v0.p, v1.p);
+    size_t tmp = 0;
+    CK(cub::DeviceRadixSort::SortPairs(nullptr, tmp, dk, dv, (int64_t)V, 0, 32, c->stream), "init_model: sort");
+    CK(c->cub_tmp.ensure(tmp), "init_model: sort scratch");
+    CK(cub::DeviceRadixSort::SortPairs(c->cub_tmp.p, tmp, dk, dv, (int64_t)V, 0, 32, c->stream), "init_model: sort");
+    CK(cudaMemcpyAsync(order.data(), dv.Current(), 4 * (size_t)V, cudaMemcpyDeviceToHost, c->stream), "init_model");
+    CK(cudaStreamSynchronize(c->stream), "init_model");
+  }
   long long size = V, tw = 0;
   for (uint32_t i = 0; i < V; i++) {
     if ((long long)c->h_deg[order[i]] < c->o.min_count && i != 0) size--;
@@ -1094,9 +1348,11 @@ extern "C" felog_status felog_init_model(felog_ctx *c) {
   c->train_words = tw;
   std::vector<long long> cn(size);
   for (long long i = 0; i < size; i++) cn[i] = c->h_deg[order[i]];
-  // unigram table (word2vec.cu:674-694)
-  std::vector<int32_t> table(kTableSize);
-  {
+  CK(c->id2offset.ensure(V), "init_model");
+  CK(cudaMemcpy(c->id2offset.p, c->h_id2offset.data(), 4 * (size_t)V, cudaMemcpyHostToDevice), "init_model");
+  if (size <= kRefTableMaxVocab) {
+    // unigram table (word2vec.cu:674-694): the reference's 1e8 slots, sequential FP64 walk
+    std::vector<int32_t> table(kTableSize);
     double twp = 0, d1, power = 0.75;
     long long i = 0;
     for (long long a = 0; a < size; a++) twp += pow((double)cn[a], power);
@@ -1109,7 +1365,34 @@ extern "C" felog_status felog_init_model(felog_ctx *c) {
       }
       if (i >= size) i = size - 1;
     }
+    c->table_size = kTableSize;
+    CK(c->table.ensure(kTableSize), "init_model: unigram table");
+    CK(cudaMemcpy(c->table.p, table.data(), 4 * (size_t)kTableSize, cudaMemcpyHostToDevice), "init_model");
+  } else {
+    // larger vocabularies: 1e8 slots would leave most words without a slot, so
+    // the table has the power of two >= 8 x vocabulary slots, slot a holding
+    // the first word whose cumulative degree^0.75 exceeds (a + 1/2) / slots of
+    // the total (built on the device; a deviation from word2vec.cu:171)
+    uint64_t T = 1;
+    while (T < 8ull * (uint64_t)size) T <<= 1;
+    if (T > 0x80000000ull) return fail(c, FELOG_INVALID_ARG, "init_model: vocabulary too large for the unigram table");
+    DevBuf<double> wcum;
+    CK(wcum.ensure(size), "init_model: unigram weights");
+    k_unigram_weights<<<grid_for(c, size, 256), 256, 0, c->stream>>>(c->deg.p, c->id2offset.p, V, wcum.p);
+    c->launches++;
+    size_t tmp = 0;
+    CK(cub::DeviceScan::InclusiveSum(nullptr, tmp, wcum.p, wcum.p, (int64_t)size, c->stream), "init_model: scan");
+    CK(c->cub_tmp.ensure(tmp), "init_model: scan scratch");
+    CK(cub::DeviceScan::InclusiveSum(c->cub_tmp.p, tmp, wcum.p, wcum.p, (int64_t)size, c->stream),
+       "init_model: scan");
+    c->table_size = T;
+    CK(c->table.ensure(T), "init_model: unigram table");
+    k_unigram_fill<<<grid_for(c, T, 256), 256, 0, c->stream>>>(wcum.p, (uint64_t)size, T, c->table.p);
+    c->launches++;
+    CK(cudaGetLastError(), "init_model: unigram table");
+    CK(cudaStreamSynchronize(c->stream), "init_model");
   }
+  c->cub_tmp.release();
   // subsampling thresholds (word2vec.cu:180-212)
   std::vector<uint16_t> thr;
   {
@@ -1135,14 +1418,10 @@ extern "C" felog_status felog_init_model(felog_ctx *c) {
     et[i] = expf((i / (float)1000 * 2 - 1) * 6);
     et[i] = et[i] / (et[i] + 1);
   }
-  CK(c->id2offset.ensure(V), "init_model");
-  CK(cudaMemcpy(c->id2offset.p, c->h_id2offset.data(), 4 * (size_t)V, cudaMemcpyHostToDevice), "init_model");
-  CK(c->table.ensure(kTableSize), "init_model: unigram table");
-  CK(cudaMemcpy(c->table.p, table.data(), 4 * (size_t)kTableSize, cudaMemcpyHostToDevice), "init_model");
   {
-    const uint64_t nb = ((uint64_t)kTableSize + 63) >> kCoarseShift;
+    const uint64_t nb = (c->table_size + 63) >> kCoarseShift;
     CK(c->table_coarse.ensure(nb), "init_model: unigram buckets");
-    k_unigram_coarse<<<grid_for(c, nb, 256), 256, 0, c->stream>>>(c->table.p, kTableSize, c->table_coarse.p);
+    k_unigram_coarse<<<grid_for(c, nb, 256), 256, 0, c->stream>>>(c->table.p, c->table_size, c->table_coarse.p);
     c->launches++;
     CK(cudaGetLastError(), "init_model: unigram buckets");
   }
@@ -1233,7 +1512,7 @@ felog_status plan_round(felog_ctx *c, float *ms) {
   a.id2offset = c->id2offset.p;
   a.thr = c->use_thr ? c->thr.p : nullptr;
   a.table = c->table.p;
-  a.table_size = kTableSize;
+  a.table_size = c->table_size;
   a.vocab_size = c->vocab_size;
   a.negative = c->o.negative;
   a.seed = 0x9E3779B97F4A7C15ULL ^ ((0ULL + 1ULL) << 1) ^ 0x2ULL;  // InitSeedForRank(0, 2), word2vec.cu:146-152
@@ -1344,6 +1623,7 @@ felog_status train_pairs(felog_ctx *c, SgArgs g, int blocks, int threads) {
   pa.table = c->table.p;
   pa.fm_window = g.fm_window;
   pa.fm_vocab1 = g.fm_vocab1;
+  pa.fm_table = make_fastmod((uint32_t)c->table_size);
   pa.window = c->o.window;
   pa.negative = K;
   pa.stride = stride;
@@ -1524,7 +1804,7 @@ extern "C" felog_status felog_train_round(felog_ctx *c, uint32_t round, float al
   g.negs = c->p_negs.p;
   g.n_sent = c->plan_sent;
   g.table = c->table.p;
-  g.table_size = kTableSize;
+  g.table_size = c->table_size;
   g.vocab_size = c->vocab_size;
   g.exp_table = c->exp_table.p;
   g.window = c->o.window;
@@ -1538,6 +1818,8 @@ extern "C" felog_status felog_train_round(felog_ctx *c, uint32_t round, float al
   g.syn1_bf = c->syn1_bf.p;
   g.n_hot = c->n_f32;
   g.sr_seed = sr_hash((uint32_t)c->o.seed ^ sr_hash((uint32_t)(c->o.seed >> 32) + round * 0x9E3779B9u));
+  // a streamed round trains its pieces one by one; each piece gets its own rounding seed
+  if (c->chunk_base) g.sr_seed = sr_hash(g.sr_seed ^ sr_hash(c->chunk_base));
   {
     // negative-draw LCG x -> 25214903917 x + 11 (word2vec.cu:502) composed q + 1 times
     unsigned long long A = 1, C = 0;
@@ -2430,21 +2712,34 @@ extern "C" felog_status felog_run(felog_ctx *c, felog_run_stats *st) {
   const uint32_t min_r = c->o.min_rounds ? c->o.min_rounds : 1;
   for (uint32_t r = 0;; r++) {
     if (c->o.max_rounds > 0 && (int)r >= c->o.max_rounds) break;
-    felog_walk_stats ws;
-    s = felog_walk_round(c, r, nullptr, &ws);
+    // the round's walkers, whole or in pieces of stream_walkers: walk a piece,
+    // train on its corpus, go on (walks depend on the graph and the stop flags
+    // only, so the pieces walk exactly what the whole round would)
+    s = walk_prepare(c);
     if (s != FELOG_OK) return s;
-    if (c->o.budget_mode == FELOG_BUDGET_LEARNED && !c->pred_ready) {
-      s = felog_mlp_predict(c, nullptr, nullptr, nullptr);  // features from the first round's walks
+    const uint32_t na = c->n_active;
+    const uint32_t piece = c->o.stream_walkers ? c->o.stream_walkers : std::max<uint32_t>(na, 1);
+    for (uint32_t k0 = 0; k0 < na || k0 == 0; k0 += piece) {
+      const uint32_t k1 = std::min<uint64_t>((uint64_t)k0 + piece, na);
+      c->chunk_base = k0;
+      felog_walk_stats ws;
+      s = walk_range(c, r, nullptr, k0, k1, &ws, k1 == na);
       if (s != FELOG_OK) return s;
+      rs.walk_tokens += ws.n_tokens;
+      rs.walk_ms += ws.ms;
+      if (c->o.budget_mode == FELOG_BUDGET_LEARNED && !c->pred_ready && k1 == na) {
+        s = felog_mlp_predict(c, nullptr, nullptr, nullptr);  // features from the first round's walks
+        if (s != FELOG_OK) return s;
+      }
+      felog_train_stats ts;
+      s = felog_train_round(c, r, -1.0f, &ts);
+      if (s != FELOG_OK) return s;
+      rs.train_words += ts.words;
+      rs.train_ms += ts.ms_plan + ts.ms_train;
+      if (k1 >= na) break;
     }
-    felog_train_stats ts;
-    s = felog_train_round(c, r, -1.0f, &ts);
-    if (s != FELOG_OK) return s;
+    c->chunk_base = 0;
     rs.rounds = r + 1;
-    rs.walk_tokens += ws.n_tokens;
-    rs.train_words += ts.words;
-    rs.walk_ms += ws.ms;
-    rs.train_ms += ts.ms_plan + ts.ms_train;
     if (r + 1 >= min_r) {  // train_iter >= init_round, word2vec.cu:2011-2017
       felog_budget_stats bs;
       s = felog_budget_check(c, r, &bs);

@@ -38,6 +38,7 @@ struct PairArgs {
   const int32_t *table;
   FastMod fm_window;
   FastMod fm_vocab1;
+  FastMod fm_table;      // % unigram table slots
   int window;
   int negative;
   int stride;
@@ -181,7 +182,7 @@ __global__ void __launch_bounds__(256) k_pair_emit(PairArgs a) {
 #pragma unroll
           for (int u = 0; u < U; u++) {
             nr[u] = nr[u] * 25214903917ULL + 11ULL;
-            t[u][q] = unigram_lookup(a.table, a.coarse, (nr[u] >> 16) % kUnigramSlots);
+            t[u][q] = unigram_lookup(a.table, a.coarse, fastmod(nr[u] >> 16, a.fm_table));
             if (t[u][q] == 0) t[u][q] = -2 - (int)fastmod(nr[u], a.fm_vocab1);  // fallback, resolved below
           }
       }

@@ -44,7 +44,7 @@ class FelogOpts(ctypes.Structure):
         ("device", ctypes.c_int32), ("slot_len", ctypes.c_int32), ("seed", ctypes.c_uint64),
         ("long_arena_tokens", ctypes.c_uint64), ("wait_limit", ctypes.c_uint64),
         ("hot_rows", ctypes.c_int64), ("budget_confidence", ctypes.c_float), ("budget_audit", ctypes.c_float),
-        ("autotune", ctypes.c_int32),
+        ("autotune", ctypes.c_int32), ("stream_walkers", ctypes.c_uint32),
     ]
 
 
@@ -96,6 +96,17 @@ class RunStats(ctypes.Structure):
                 ("overruled", ctypes.c_uint64)]
 
 
+class RmatParams(ctypes.Structure):
+    _fields_ = [("seed", ctypes.c_uint64), ("v_target", ctypes.c_uint64), ("e_target", ctypes.c_uint64),
+                ("a", ctypes.c_double), ("b", ctypes.c_double), ("c", ctypes.c_double), ("d", ctypes.c_double),
+                ("lognormal", ctypes.c_int32), ("lognormal_mu", ctypes.c_double),
+                ("lognormal_sigma", ctypes.c_double), ("permute_ids", ctypes.c_int32)]
+
+
+class RmatInfo(ctypes.Structure):
+    _fields_ = [("v_num", ctypes.c_uint32), ("n_edges", ctypes.c_uint64), ("max_degree", ctypes.c_uint32)]
+
+
 def _struct_dict(s):
     return {k: getattr(s, k) for k, _ in s._fields_}
 
@@ -130,6 +141,7 @@ def gpu_lib():
         L.felog_last_error.restype = ctypes.c_char_p
         L.felog_load_graph.argtypes = [_P, _P, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_int]
         L.felog_load_graph_file.argtypes = [_P, ctypes.c_char_p, ctypes.c_uint32, ctypes.c_int]
+        L.felog_load_rmat.argtypes = [_P, ctypes.POINTER(RmatParams), ctypes.c_int, ctypes.POINTER(RmatInfo)]
         L.felog_graph_info.argtypes = [_P, _P, _P]
         L.felog_get_csr.argtypes = [_P, _P, _P, _P]
         L.felog_get_degrees.argtypes = [_P, _P]
@@ -139,6 +151,8 @@ def gpu_lib():
         L.felog_get_stop_flags.argtypes = [_P, _P]
         L.felog_walk_round.argtypes = [_P, ctypes.c_uint32, ctypes.POINTER(Draws), ctypes.POINTER(WalkStats)]
         L.felog_corpus_size.argtypes = [_P, _P, _P]
+        L.felog_walk_piece.argtypes = [_P, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint64, _P,
+                                       ctypes.POINTER(WalkStats)]
         L.felog_get_corpus.argtypes = [_P, _P, ctypes.c_uint64, _P, ctypes.c_uint64]
         L.felog_set_corpus.argtypes = [_P, _P, _P, ctypes.c_uint64]
         L.felog_get_visit_freq.argtypes = [_P, _P]
@@ -254,6 +268,15 @@ class Felog:
         e = np.ascontiguousarray(edges, dtype=EDGE12)
         self._ck(self._L.felog_load_graph(self.h, _addr(e), len(e), v_num, int(undirected)))
 
+    def load_rmat(self, seed, v_target, e_target, abcd=(0.57, 0.19, 0.19, 0.05), lognormal=False, permute=True,
+                  mu=0.0, sigma=1.0, undirected=True):
+        """felog_load_rmat: the seeded R-MAT graph generated and loaded on the device
+        (the edges of synth_graph(..., holdout=0)); returns its info."""
+        p = RmatParams(seed, v_target, e_target, *abcd, 1 if lognormal else 0, mu, sigma, int(permute))
+        info = RmatInfo()
+        self._ck(self._L.felog_load_rmat(self.h, ctypes.byref(p), int(undirected), ctypes.byref(info)))
+        return _struct_dict(info)
+
     def load_graph_file(self, path, v_num, undirected=True):
         self._ck(self._L.felog_load_graph_file(self.h, path.encode(), v_num, int(undirected)))
 
@@ -311,6 +334,14 @@ class Felog:
         self._ck(self._L.felog_walk_round(self.h, round_, ctypes.byref(dr) if dr is not None else None,
                                           ctypes.byref(st)))
         return _struct_dict(st)
+
+    def walk_piece(self, round_, first, count):
+        """felog_walk_piece: active walkers first .. first + count - 1 of the round walk; returns
+        (stats, number of active walkers of the round)."""
+        st = WalkStats()
+        na = ctypes.c_uint64()
+        self._ck(self._L.felog_walk_piece(self.h, round_, first, count, ctypes.byref(na), ctypes.byref(st)))
+        return _struct_dict(st), na.value
 
     def common_neighbours(self, src, dst, v_num, undirected=True):
         """felog_common_neighbours: per input edge, the common-neighbour count

@@ -100,3 +100,36 @@ def tables_by_vertex(f):
     _, id2, vs, _ = f.vocab()
     dim = f.opts.size
     return s0.reshape(vs, dim)[id2], s1.reshape(vs, dim)[id2]
+
+
+def fit_pairs(g, n=20000, seed=12345):
+    """Evaluation pairs of the fit score: n training edges (u, v) as positives
+    and, for each, a negative (u, w) with w an endpoint of a uniformly chosen
+    training edge (so w is drawn in proportion to its degree, like the
+    positives' endpoints) that is neither u nor a neighbour of u.  Returns
+    (src, dst, label)."""
+    src = g["edges"]["src"].astype(np.int64)
+    dst = g["edges"]["dst"].astype(np.int64)
+    rng = np.random.default_rng(seed)
+    lo, hi = np.minimum(src, dst), np.maximum(src, dst)
+    known = set((lo << 32 | hi).tolist())
+    ts, td = g["test_src"].astype(np.int64), g["test_dst"].astype(np.int64)
+    p = g["test_label"] == 1
+    known |= set((np.minimum(ts[p], td[p]) << 32 | np.maximum(ts[p], td[p])).tolist())
+    ends = np.concatenate([src, dst])
+    m = rng.choice(len(src), min(n, len(src)), replace=False)
+    us, vs = src[m], dst[m]
+    ws = np.empty_like(us)
+    for i, u in enumerate(us.tolist()):
+        while True:
+            w = int(ends[rng.integers(len(ends))])
+            if w != u and (min(u, w) << 32 | max(u, w)) not in known:
+                break
+        ws[i] = w
+    return (np.concatenate([us, us]), np.concatenate([vs, ws]),
+            np.concatenate([np.ones(len(us), np.uint8), np.zeros(len(us), np.uint8)]))
+
+
+def fit_aucs(syn0, syn1, pairs):
+    s, d, lab = pairs
+    return {k: auc(v, lab) for k, v in link_scores(syn0, syn1, s, d).items()}

@@ -36,7 +36,7 @@ def test_default_opts_follow_reference_defaults():
     assert abs(o.sample - 1e-3) < 1e-9 and abs(o.alpha - 0.025) < 1e-9
     assert (o.min_length, o.min_rounds, o.eval_batch_size) == (20, 5, 16384)
     # the Python mirror of felog_opts matches the C layout to its last field
-    assert ctypes.sizeof(fb.FelogOpts) == 160
+    assert ctypes.sizeof(fb.FelogOpts) == 160 and fb.FelogOpts.stream_walkers.offset == 156
     assert (o.seed, o.slot_len, o.hot_rows, o.autotune) == (0x5EED0001, 64, 0, 1)
     assert o.budget_confidence == 0.0 and o.budget_audit == 0.0
 
@@ -49,7 +49,7 @@ def test_create_reports_status_without_crashing():
     assert st in (0, 3)
     if st == 0:
         L.felog_destroy(h)
-    assert L.felog_abi_version() == 2
+    assert L.felog_abi_version() == 3
 
 
 def test_synth_graph_contract():

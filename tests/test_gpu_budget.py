@@ -101,3 +101,27 @@ def test_async_embedding_copy_equals_sync_copy():
     f.embeddings_into_async(ctypes.c_void_p(buf.data_ptr()), vs * 128)
     f.wait_embeddings()
     np.testing.assert_array_equal(buf.numpy(), sync1)
+
+
+def test_streamed_rounds_walk_the_same_corpus():
+    """felog_run with stream_walkers walks and trains each round in pieces: the
+    walks are the same as in whole rounds (they depend on the graph and the
+    stop flags only), each piece is planned and trained on its own, and the
+    embedding reaches the same fit quality."""
+    import ref_tables as rt
+
+    g = fb.synth_graph(seed=0, v_target=16384, e_target=131072, holdout=0.10)
+    V = g["v_num"]
+    pairs = rt.fit_pairs(g)
+    res = {}
+    for piece in (0, 3000):
+        f = fb.Felog(v_num=V, size=128, window=10, negative=5, cbow=0, reuse_neg=0, min_count=0, min_rounds=2,
+                     max_rounds=2, seed=11, stream_walkers=piece)
+        f.load_graph(g["edges"], V)
+        rs = f.run()
+        res[piece] = (rs, rt.fit_aucs(*rt.tables_by_vertex(f), pairs)["cosine_centered"])
+        f.close()
+    (a, qa), (b, qb) = res[0], res[3000]
+    assert a["rounds"] == b["rounds"] == 2
+    assert a["walk_tokens"] == b["walk_tokens"] and a["train_words"] == b["train_words"]
+    assert qa > 0.7 and abs(qa - qb) < 0.02, (qa, qb)
