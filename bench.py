@@ -58,6 +58,18 @@ CONFIGS = {
                seed=0, v_target=16384, e_target=131072, abcd=(0.57, 0.19, 0.19, 0.05), lognormal=False,
                holdout=0.10),
 }
+# Configurations too large for a host edge list: the graph is generated on the
+# device (felog_load_rmat, the same edges the host generator would draw, no
+# held-out split) and every round is walked and trained in pieces of `piece`
+# walkers (a step of the benchmark is one piece).
+STREAMED = {
+    "c5": dict(workload="learned-bf16, seed-3 R-MAT (.57/.19/.19/.05) 111M vertex ids / 1.6B undirected edges, "
+                        "weights uniform in (0, 1], generated on the device",
+               seed=3, v_target=111_000_000, e_target=1_600_000_000, abcd=(0.57, 0.19, 0.19, 0.05), piece=8_000_000),
+    "c5-small": dict(workload="learned-bf16, seed-3 R-MAT (.57/.19/.19/.05) 4M vertex ids / 60M undirected edges "
+                              "(the C5 path at 1/27 scale), generated on the device",
+                     seed=3, v_target=4_000_000, e_target=60_000_000, abcd=(0.57, 0.19, 0.19, 0.05), piece=1_000_000),
+}
 TRAIN = dict(min_length=20, min_rounds=2, size=128, window=10, negative=5, sample=1e-3, cbow=0, reuse_neg=0,
              min_count=0)
 FORMS = {
@@ -473,6 +485,129 @@ def bench_mine(args):
         pg.destroy_process_group()
 
 
+def bench_streamed(args):
+    """Streamed configuration (C5): one step = one piece of a round (walk the
+    piece's walkers, plan and train on their corpus), inputs resident in HBM.
+    e2e = one whole job through the C ABI (device generation from a parameter
+    block, felog_run to the stop-all rule, syn0 copied to host memory);
+    forms = plain FP32 and learned BF16 jobs on the same graph."""
+    import felog_b200 as fb
+    cfg = STREAMED[args.config]
+    model = np.load(args.budget_model)
+    piece = cfg["piece"]
+
+    def context(form):
+        f = fb.Felog(v_num=cfg["v_target"], device=0, seed=1000, autotune=0 if args.no_autotune else 1,
+                     stream_walkers=piece, **{**TRAIN, **FORMS[form]})
+        t0 = time.perf_counter()
+        info = f.load_rmat(cfg["seed"], cfg["v_target"], cfg["e_target"], abcd=cfg["abcd"])
+        gen_s = time.perf_counter() - t0
+        f.init_model()
+        if FORMS[form]["budget_mode"] == 1:
+            f.mlp_set_state(model)
+        return f, info, gen_s
+
+    form = args.form
+    prec = "bf16" if FORMS[form]["precision"] else "fp32"
+    f, info, gen_s = context(form)
+    log(f"graph: {info} generated and loaded in {gen_s:.1f}s")
+    V = info["v_num"]
+    state = {"round": 0, "first": 0, "na": None}
+
+    def step(acc):
+        ws, na = f.walk_piece(state["round"], state["first"], piece)
+        ts = f.train_round(state["round"])
+        state["first"] += piece
+        if state["first"] >= na:
+            state["round"] += 1
+            state["first"] = 0
+        for k, v in (("tokens", ws["n_tokens"]), ("words", ts["words"]), ("pairs", ts["pairs"]),
+                     ("kept", ts["kept_words"]), ("walk_ms", ws["ms"]), ("train_ms", ts["ms_train"]),
+                     ("plan_ms", ts["ms_plan"])):
+            acc[k] = acc.get(k, 0.0) + v
+
+    warm = {}
+    for _ in range(args.warmup):
+        step(warm)
+    log(f"warmup done: {warm}")
+    cnt = {}
+    launches0 = f.kernel_launches()
+    with ClockSampler(0) as clk:
+        f.timer_mark(0)
+        for _ in range(args.steps):
+            step(cnt)
+        f.timer_mark(1)
+        ms = f.timer_elapsed()
+    launches = f.kernel_launches() - launches0
+    mix_pairs, mix_refs, mix_hot = f.pair_row_mix()
+    refs_per_pair = mix_refs / mix_pairs
+    hot_share = mix_hot / mix_refs
+    per_ref = 2 * (512 * hot_share + 256 * (1 - hot_share)) if prec == "bf16" else 2 * 512
+    peak, peak_kind = measured_peaks()
+    sg_achieved = cnt["pairs"] * refs_per_pair * per_ref / (cnt["train_ms"] * 1e-3) / 1e9
+    walk_achieved = cnt["tokens"] * WALK_BYTES_PER_STEP / (cnt["walk_ms"] * 1e-3) / 1e9
+    # ---- e2e: a whole job through the C ABI, host buffers (syn0 back to host memory)
+    vs = f.vocab()[2]
+    emb = np.empty(vs * TRAIN["size"], np.float32)
+    f.init_model()
+    if FORMS[form]["budget_mode"] == 1:
+        f.mlp_set_state(model)
+    t0 = time.perf_counter()
+    job = f.run()
+    f.embeddings_into(emb.ctypes.data, emb.size)
+    e2e_s = time.perf_counter() - t0
+    f.close()
+    del emb
+    out = {
+        "metric": METRIC, "value": cnt["tokens"] / (ms * 1e-3), "unit": "tokens/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": ("f32 tables" if prec == "fp32" else "bf16 tables (f32 master rows for the top 1%), f32 arithmetic")
+                 + ", f64 walk statistics",
+        "data": "synthetic (seeded R-MAT generated on the device, see config)",
+        "config": {"workload": cfg["workload"].replace("learned-bf16", form), "form": form, "v_num": V,
+                   "undirected_edges": info["n_edges"], "max_degree": info["max_degree"], "dim": 128, "window": 10,
+                   "negative": 5, "sample": 1e-3, "min_L": 20, "min_R": 2, "skip_gram": True, "precision": prec,
+                   "step": f"one piece of {piece} walkers of a round: walk, plan, pair stream, train",
+                   "unigram_table_slots": "2^30 (8 per word; the reference's 1e8 below 12.5M words)",
+                   "l2": "inputs larger than L2", "parallelism": "replicas x1", "graph_gen_s": gen_s},
+        "walk_steps_per_s": cnt["tokens"] / (cnt["walk_ms"] * 1e-3),
+        "sgns_words_per_s": cnt["words"] / ((cnt["train_ms"] + cnt["plan_ms"]) * 1e-3),
+        "phase_ms_per_step": {k: cnt[k] / args.steps for k in ("walk_ms", "plan_ms", "train_ms")},
+        "tokens_per_step": cnt["tokens"] / args.steps, "pairs_per_step": cnt["pairs"] / args.steps,
+        "roofline": {"kernel": f"k_sgns_train_pairs<128, 5, Rows{prec.upper()}>", "bound": "hbm",
+                     "traffic": DRAM_BYTES_PER_PAIR[prec] * cnt["pairs"] / args.steps,
+                     "traffic_unit": "bytes per step (ncu per-pair DRAM traffic of the profiling case x pairs)",
+                     "achieved": sg_achieved, "peak": peak, "unit": "GB/s", "frac": sg_achieved / peak,
+                     "algorithmic_bytes_per_pair": refs_per_pair * per_ref, "row_refs_per_pair": refs_per_pair,
+                     "master_row_share": hot_share, "peak_source": peak_kind,
+                     "walk_kernel": {"achieved": walk_achieved, "frac": walk_achieved / peak,
+                                     "bytes_per_step": WALK_BYTES_PER_STEP}},
+        "e2e": {"value": job["walk_tokens"] / e2e_s, "unit": "tokens/s", "h2d_bytes_per_step": 120,
+                "d2h_bytes_per_step": int(vs * TRAIN["size"] * 4),
+                "what": "one whole job per step: device generation from the parameter block, felog_run to the "
+                        "stop-all rule, syn0 copied to host memory", "rounds": job["rounds"], "job_s": e2e_s},
+        "gpu_launches": int(launches),
+        "clocks": clk.summary(),
+    }
+    if not args.no_forms:
+        forms = {}
+        for fm in ("plain-fp32", "learned-bf16"):
+            g2, _, gs = context(fm)
+            t0 = time.perf_counter()
+            rs = g2.run()
+            wall = time.perf_counter() - t0
+            forms[fm] = {"rounds": rs["rounds"], "walk_tokens": rs["walk_tokens"], "train_words": rs["train_words"],
+                         "job_ms": rs["total_ms"], "wall_ms": wall * 1e3,
+                         "tokens_per_s": rs["walk_tokens"] / (rs["total_ms"] * 1e-3),
+                         "budget": {k: rs[k] for k in ("evaluated", "predicted", "audited", "overruled")}}
+            g2.close()
+        forms["learned-bf16"]["end_to_end_speedup_vs_plain_fp32"] = (forms["plain-fp32"]["job_ms"]
+                                                                     / forms["learned-bf16"]["job_ms"])
+        out["forms"] = forms
+    print(json.dumps(out), flush=True)
+
+
 def bench_reference(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -578,7 +713,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
-    ap.add_argument("--config", default="c2", choices=sorted(CONFIGS))
+    ap.add_argument("--config", default="c2", choices=sorted(CONFIGS) + sorted(STREAMED))
     ap.add_argument("--ref-walkers", type=int, default=0,
                     help="walkers of the reference arm (0: one per vertex; the reference asserts every vertex is visited)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -600,6 +735,13 @@ def main():
         return
     if args.workload == "gcn":
         bench_gcn(args)
+    elif args.config in STREAMED:
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the reference's CPU walk engine needs about 15 min "
+                              "per round at 111M vertices (2.6 M steps/s on 16 threads, 2.4 G steps per round) and "
+                              "its graph load a host edge list of 19 GB; bench it at c2"}))
+        else:
+            bench_streamed(args)
     elif args.impl == "reference":
         bench_reference(args)
     else:

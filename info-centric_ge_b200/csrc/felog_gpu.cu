@@ -1922,12 +1922,13 @@ extern "C" felog_status felog_get_plan(felog_ctx *c, int32_t *sen, uint64_t *sen
 namespace {
 
 // interleaved rows -> logical order (see sgns.cuh); rows n_f32.. from BF16
+// rows r0 .. r0 + rows - 1 into dst (row r0 first)
 __global__ void k_unpermute(const float *src, const uint16_t *src_bf, uint64_t n_f32, float *dst, uint64_t rows,
-                            int dim) {
+                            int dim, uint64_t r0 = 0) {
   const int Jn = dim / 32;
   const uint64_t n = rows * (uint64_t)dim;
   for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < n; e += (uint64_t)gridDim.x * blockDim.x) {
-    uint64_t r = e / dim;
+    uint64_t r = r0 + e / dim;
     int l = (int)(e % dim);
     const uint64_t col = (uint64_t)(l % 32) * Jn + l / 32;
     dst[e] = r < n_f32 ? src[r * dim + col] : __uint_as_float((uint32_t)src_bf[(r - n_f32) * dim + col] << 16);
@@ -1943,18 +1944,23 @@ extern "C" felog_status felog_get_embeddings(felog_ctx *c, float *syn0, float *s
   const uint64_t nel = (uint64_t)c->vocab_size * dim;
   if (cap_floats < nel) return fail(c, FELOG_INVALID_ARG, "get_embeddings: need %llu floats", (unsigned long long)nel);
   CK(cudaSetDevice(c->device), "get_embeddings");
-  CK(c->out_tmp.ensure(nel), "get_embeddings");
+  // staged through at most 1 GiB of device memory at a time
+  const uint64_t step = std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)c->vocab_size, (1ull << 28) / dim));
+  CK(c->out_tmp.ensure(std::min<uint64_t>(nel, step * dim)), "get_embeddings");
   for (int which = 0; which < 2; which++) {
     float *dst = which ? syn1 : syn0;
     if (!dst) continue;
-    k_unpermute<<<grid_for(c, nel, 256), 256, 0, c->stream>>>(which ? c->syn1.p : c->syn0.p,
-                                                               which ? c->syn1_bf.p : c->syn0_bf.p,
-                                                               (uint64_t)c->n_f32, c->out_tmp.p,
-                                                               (uint64_t)c->vocab_size, dim);
-    c->launches++;
-    CK(cudaGetLastError(), "get_embeddings");
-    CK(cudaMemcpyAsync(dst, c->out_tmp.p, 4 * nel, cudaMemcpyDeviceToHost, c->stream), "get_embeddings");
-    CK(cudaStreamSynchronize(c->stream), "get_embeddings");
+    for (uint64_t r0 = 0; r0 < (uint64_t)c->vocab_size; r0 += step) {
+      const uint64_t nr = std::min<uint64_t>(step, (uint64_t)c->vocab_size - r0);
+      k_unpermute<<<grid_for(c, nr * dim, 256), 256, 0, c->stream>>>(which ? c->syn1.p : c->syn0.p,
+                                                                    which ? c->syn1_bf.p : c->syn0_bf.p,
+                                                                    (uint64_t)c->n_f32, c->out_tmp.p, nr, dim, r0);
+      c->launches++;
+      CK(cudaGetLastError(), "get_embeddings");
+      CK(cudaMemcpyAsync(dst + r0 * dim, c->out_tmp.p, 4 * nr * dim, cudaMemcpyDeviceToHost, c->stream),
+         "get_embeddings");
+      CK(cudaStreamSynchronize(c->stream), "get_embeddings");
+    }
   }
   return FELOG_OK;
 }
