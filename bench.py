@@ -201,24 +201,6 @@ def sum_over_ranks(pg, x):
     return float(t.item())
 
 
-def run_round(f, r, min_rounds, counters):
-    ws = f.walk_round(r)
-    if f.opts.budget_mode == 1 and r == 0:
-        f.mlp_predict()  # learned budget: features from the first round's walks
-    ts = f.train_round(r)
-    counters["tokens"] += ws["n_tokens"]
-    counters["words"] += ts["words"]
-    counters["pairs"] += ts["pairs"]
-    counters["kept"] += ts["kept_words"]
-    counters["walk_ms"] += ws["ms"]
-    counters["last_walk"] = (ws["n_tokens"], ws["ms"])
-    counters["train_ms"] += ts["ms_train"]
-    counters["plan_ms"] += ts["ms_plan"]
-    if r + 1 >= min_rounds:
-        bs = f.budget_check(r)
-        counters["budget_ms"] += bs["ms"]
-
-
 def cpu_baseline(g, cfg):
     """The oracle (CPU restatement) on a bounded sample of the workload: the walk
     of 60k walkers and the skip-gram pass over their first 1500 sentences,
@@ -339,75 +321,80 @@ def bench_mine(args):
     prec = "bf16" if FORMS[form]["precision"] else "fp32"
     model = np.load(args.budget_model) if FORMS[form]["budget_mode"] or not args.no_forms else None
     f = new_context(fb, g, form, local, 1000 + rank, model, autotune=0 if args.no_autotune else 1)
-    min_r = TRAIN["min_rounds"]
-    warm = {k: 0.0 for k in ("tokens", "words", "pairs", "kept", "walk_ms", "train_ms", "plan_ms", "budget_ms")}
-    for r in range(args.warmup):
-        run_round(f, r, min_r, warm)
+    keys = ("tokens", "words", "pairs", "walk_ms", "train_ms", "plan_ms", "budget_ms", "rounds")
+
+    def job(acc, timed=False):
+        """One whole job: InitNet, then walk / train / budget-check rounds until
+        the stop-all rule (felog_run).  timed: the device time of the rounds
+        (InitNet, the vocabulary and the unigram table excluded) is added to
+        acc["ms"]."""
+        f.init_model()
+        if timed:
+            f.timer_mark(0)
+        rs = f.run()
+        if timed:
+            f.timer_mark(1)
+            acc["ms"] = acc.get("ms", 0.0) + f.timer_elapsed()
+        for k, v in (("tokens", rs["walk_tokens"]), ("words", rs["train_words"]), ("pairs", rs["pairs"]),
+                     ("walk_ms", rs["walk_ms"]), ("train_ms", rs["train_ms"] - rs["plan_ms"]),
+                     ("plan_ms", rs["plan_ms"]), ("budget_ms", rs["budget_ms"]), ("rounds", rs["rounds"])):
+            acc[k] = acc.get(k, 0.0) + v
+
+    warm = {}
+    for _ in range(args.warmup):
+        job(warm)
     log(f"warmup done: {warm}")
-    # ---- device-timed region: inputs resident in HBM
+    # ---- device-timed region: whole jobs, inputs resident in HBM
     if pg is not None:
         pg.barrier()
-    cnt = {k: 0.0 for k in warm}
+    cnt = {}
     launches0 = f.kernel_launches()
     with ClockSampler(local) as clk:
-        f.timer_mark(0)
-        for r in range(args.warmup, args.warmup + args.steps):
-            run_round(f, r, min_r, cnt)
-        f.timer_mark(1)
-        ms = f.timer_elapsed()
+        for _ in range(args.steps):
+            job(cnt, timed=True)
+    ms = cnt["ms"]
     launches = f.kernel_launches() - launches0
     # the walker against the attainable rate of its own access pattern: the
-    # memory skeleton of the last timed round (same walkers and lengths,
-    # dependent uniform-neighbour gathers, no arithmetic), timed outside the
-    # timed region
+    # memory skeleton of the last round (same walkers and lengths, dependent
+    # uniform-neighbour gathers, no arithmetic), timed outside the timed region
     ceil_ms, ceil_tok = f.walk_ceiling()
-    last_tok, last_ms = cnt["last_walk"]
     ms_max = max_over_ranks(pg, ms)
     tokens_all = sum_over_ranks(pg, cnt["tokens"])
     value = tokens_all / (ms_max * 1e-3)
-    # ---- end to end through the C ABI with host buffers
-    import ctypes
-
+    # ---- end to end through the C ABI with host buffers: per job the edge
+    # list goes up from pinned memory (CSR build included) and the trained
+    # syn0 comes back to pinned memory
     import torch
-    flags_h = torch.zeros(V, dtype=torch.uint8).pin_memory()
-    flags_h.numpy()[:] = f.stop_flags()
     vs = f.vocab()[2]
+    edges_h = torch.from_numpy(g["edges"].view(np.uint8)).pin_memory()
     emb_h = torch.empty(vs * 128, dtype=torch.float32).pin_memory()
-    e2e = {k: 0.0 for k in warm}
-    # the same rounds again from InitNet (same walk seed), so that both regions
-    # process the same walks; one untimed copy sets up the copy stream
-    f.init_model()
-    flags_h.numpy()[:] = 0
-    e2e_warm = dict(e2e)
+    edges_pinned = np.frombuffer(edges_h.numpy().data, dtype=g["edges"].dtype)
+    e2e = {}
 
-    def e2e_round(r, acc):
-        f.set_stop_flags_from(ctypes.c_void_p(flags_h.data_ptr()))
-        run_round(f, r, min_r, acc)
-        # the round's syn0 goes to pinned host memory while the next round runs
-        f.embeddings_into_async(ctypes.c_void_p(emb_h.data_ptr()), vs * 128)
-        flags_h.numpy()[:] = f.stop_flags()
+    def e2e_job(acc):
+        f.load_graph(edges_pinned, V)
+        job(acc)
+        f.embeddings_into(emb_h.data_ptr(), vs * 128)
 
-    for r in range(args.warmup):
-        e2e_round(r, e2e_warm)
-    f.wait_embeddings()
+    e2e_job({})
     if pg is not None:
         pg.barrier()
     f.timer_mark(0)
-    for r in range(args.warmup, args.warmup + args.steps):
-        e2e_round(r, e2e)
-    f.wait_embeddings()
+    for _ in range(args.steps):
+        e2e_job(e2e)
     f.timer_mark(1)
     e2e_ms = max_over_ranks(pg, f.timer_elapsed())
     e2e_value = sum_over_ranks(pg, e2e["tokens"]) / (e2e_ms * 1e-3)
+    last_tok, last_ms = cnt["tokens"], cnt["walk_ms"]
     peak, peak_kind = measured_peaks()
     # dominant kernel: the skip-gram pass
     row_bytes = SGNS_BYTES_PER_PAIR[prec] // 14
     if FORMS[form]["reuse_neg"] == 2:
         # center tiles: per center its contexts and the K + 1 targets, each read and written once
-        sg_bytes = 2 * row_bytes * (cnt["pairs"] + (TRAIN["negative"] + 1) * cnt["kept"])
+        sg_bytes = 2 * row_bytes * (cnt["pairs"] + (TRAIN["negative"] + 1) * cnt["words"])  # words: centers before subsampling (an upper bound)
         sg_kernel = f"k_sgns_reuse_tile<128, 5, Rows{prec.upper()}>"
     elif FORMS[form]["reuse_neg"] == 3:
-        sg_bytes = 2 * row_bytes * (cnt["pairs"] + (TRAIN["negative"] + 1) * cnt["kept"])
+        sg_bytes = 2 * row_bytes * (cnt["pairs"] + (TRAIN["negative"] + 1) * cnt["words"])  # words: centers before subsampling (an upper bound)
         sg_kernel = "k_sgns_reuse_tile_tc<128, 5>"
     else:
         # per pair: each referenced row (context + trained targets) read and
@@ -441,6 +428,10 @@ def bench_mine(args):
                    "dim": 128, "window": 10, "negative": 5, "sample": 1e-3, "min_L": 20, "min_R": 2,
                    "skip_gram": True, "reuse_neg": FORMS[form]["reuse_neg"], "precision": prec,
                    "l2": "inputs larger than L2 (CSR + tables > 126 MB)",
+                   "step": "one whole job: the rounds (walk, plan, pair stream, train, budget check from min_R "
+                           "on) from InitNet until the stop-all rule; the timed region holds the rounds (InitNet, "
+                           "vocabulary and unigram table are set up untimed before each job; e2e includes them)",
+                   "rounds_per_step": cnt["rounds"] / args.steps,
                    "parallelism": f"replicas x{world}"},
         "walk_steps_per_s": cnt["tokens"] / (cnt["walk_ms"] * 1e-3),
         "sgns_words_per_s": cnt["words"] / ((cnt["train_ms"] + cnt["plan_ms"]) * 1e-3),
@@ -462,10 +453,13 @@ def bench_mine(args):
                                                         "walk_steps_per_s": last_tok / (last_ms * 1e-3),
                                                         "frac": (last_tok / last_ms) / (ceil_tok / ceil_ms),
                                                         "what": "felog_walk_ceiling: memory skeleton of the "
-                                                                "last timed round on the same CSR"}}},
-        "e2e": {"value": e2e_value, "unit": "tokens/s", "h2d_bytes_per_step": int(V),
-                "d2h_bytes_per_step": int(vs * 128 * 4 + V), "ms_per_step": e2e_ms / args.steps,
-                "tokens_per_step": e2e["tokens"] / args.steps},
+                                                                "last round on the same CSR (the walker's rate: "
+                                                                "all timed rounds)"}}},
+        "e2e": {"value": e2e_value, "unit": "tokens/s", "h2d_bytes_per_step": int(g["edges"].nbytes),
+                "d2h_bytes_per_step": int(vs * 128 * 4), "ms_per_step": e2e_ms / args.steps,
+                "tokens_per_step": e2e["tokens"] / args.steps,
+                "what": "per step one whole job through the C ABI: the edge list from pinned host memory "
+                        "(CSR build included), felog_run to the stop-all rule, syn0 back to pinned host memory"},
         "gpu_launches": int(launches),
         "autotune": f.tuning_report(),
         "clocks": clk.summary(),

@@ -170,6 +170,8 @@ typedef struct felog_run_stats {
   uint64_t predicted;     /* learned mode: vertices decided by the MLP */
   uint64_t audited;       /* learned mode: confident predictions re-checked */
   uint64_t overruled;     /* learned mode: audited predictions the plain criterion reversed */
+  uint64_t pairs;         /* (center, context) updates trained */
+  double plan_ms;         /* the batch plans' share of train_ms */
 } felog_run_stats;
 
 /* ---- lifecycle ---- */

@@ -1002,8 +1002,8 @@ felog_status walk_ceiling_run(felog_ctx *c, DevBuf<uint32_t> &scratch, float *ms
     CK(cudaMemsetAsync(c->walk_claim.p, 0, 4, c->stream), "walk_ceiling");
     CK(cudaEventRecord(c->ev0, c->stream), "walk_ceiling");
     k_walk_skeleton<<<blocks, kWalkThreads, 0, c->stream>>>(c->row_ptr.p, c->adj.p, c->V, (uint32_t)c->n_sent,
-                                                             c->active.p, c->sent_ptr.p, c->sent_len.p, frac,
-                                                             scratch.p, c->walk_claim.p);
+                                                             c->active.p + c->chunk_base, c->sent_ptr.p, c->sent_len.p,
+                                                             frac, scratch.p, c->walk_claim.p);
     c->launches++;
     CK(cudaGetLastError(), "walk_ceiling");
     CK(cudaEventRecord(c->ev1, c->stream), "walk_ceiling");
@@ -2742,6 +2742,8 @@ extern "C" felog_status felog_run(felog_ctx *c, felog_run_stats *st) {
       if (s != FELOG_OK) return s;
       rs.train_words += ts.words;
       rs.train_ms += ts.ms_plan + ts.ms_train;
+      rs.plan_ms += ts.ms_plan;
+      rs.pairs += ts.pairs;
       if (k1 >= na) break;
     }
     c->chunk_base = 0;

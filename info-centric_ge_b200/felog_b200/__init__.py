@@ -93,7 +93,7 @@ class RunStats(ctypes.Structure):
                 ("walk_ms", ctypes.c_double), ("train_ms", ctypes.c_double), ("budget_ms", ctypes.c_double),
                 ("total_ms", ctypes.c_double), ("final_unconverged", ctypes.c_uint64),
                 ("evaluated", ctypes.c_uint64), ("predicted", ctypes.c_uint64), ("audited", ctypes.c_uint64),
-                ("overruled", ctypes.c_uint64)]
+                ("overruled", ctypes.c_uint64), ("pairs", ctypes.c_uint64), ("plan_ms", ctypes.c_double)]
 
 
 class RmatParams(ctypes.Structure):
