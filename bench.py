@@ -54,6 +54,13 @@ CONFIGS = {
                         "lognormal(0, 1) weights, 5% held out",
                seed=2, v_target=3072441, e_target=117_000_000, abcd=(0.6, 0.15, 0.15, 0.1), lognormal=True,
                holdout=0.05),
+    # C4 with the reference's offline step in front: the gcn tool's common-neighbour
+    # count of every training edge becomes its edge data (gcn.cpp:304-357), which
+    # the walker's trace test reads as cn (walk.hpp:997)
+    "c4cn": dict(workload="plain FP32, seed-2 R-MAT (.6/.15/.15/.1) 3,072,441 vertex ids / 117M undirected edges, "
+                          "edge data = common-neighbour counts (gcn tool), 5% held out",
+                 seed=2, v_target=3072441, e_target=117_000_000, abcd=(0.6, 0.15, 0.15, 0.1), lognormal=True,
+                 holdout=0.05, edge_data="cn"),
     "c1": dict(workload="plain FP32, seed-0 R-MAT 16,384 vertex ids / 131,072 undirected edges, 10% held out",
                seed=0, v_target=16384, e_target=131072, abcd=(0.57, 0.19, 0.19, 0.05), lognormal=False,
                holdout=0.10),
@@ -166,6 +173,14 @@ def make_graph(cfg):
     g = fb.synth_graph(seed=cfg["seed"], v_target=cfg["v_target"], e_target=cfg["e_target"], abcd=cfg["abcd"],
                        lognormal=cfg["lognormal"], holdout=cfg["holdout"])
     log(f"graph: {g['info']} in {time.time() - t:.1f}s")
+    if cfg.get("edge_data") == "cn":
+        f = fb.Felog(v_num=g["v_num"])
+        src = np.ascontiguousarray(g["edges"]["src"], np.uint32)
+        dst = np.ascontiguousarray(g["edges"]["dst"], np.uint32)
+        cn, ms = f.common_neighbours(src, dst, g["v_num"], True)
+        f.close()
+        g["edges"]["data"] = cn.astype(np.float32)
+        log(f"edge data: common neighbours in {ms:.1f} ms (mean {cn.mean():.2f}, max {cn.max()})")
     return g
 
 
@@ -358,6 +373,18 @@ def bench_mine(args):
     # memory skeleton of the last round (same walkers and lengths, dependent
     # uniform-neighbour gathers, no arithmetic), timed outside the timed region
     ceil_ms, ceil_tok = f.walk_ceiling()
+    # walk lengths of the last round and walks per vertex of the last job
+    lens = np.diff(f.corpus()[1].astype(np.int64))
+    wpv = f.budget_labels()[0].astype(np.int64)
+
+    def summary(x):
+        return {"mean": float(x.mean()), "min": int(x.min()), "p10": float(np.percentile(x, 10)),
+                "p50": float(np.percentile(x, 50)), "p90": float(np.percentile(x, 90)),
+                "p99": float(np.percentile(x, 99)), "max": int(x.max())}
+
+    walks = {"length_last_round": summary(lens), "walks_per_vertex_last_job": summary(wpv),
+             "what": "tokens per walk of the last round; walks a vertex made in the last job before a "
+                     "convergence check stopped it (budget labels, 2..10)"}
     ms_max = max_over_ranks(pg, ms)
     tokens_all = sum_over_ranks(pg, cnt["tokens"])
     value = tokens_all / (ms_max * 1e-3)
@@ -460,6 +487,7 @@ def bench_mine(args):
                 "tokens_per_step": e2e["tokens"] / args.steps,
                 "what": "per step one whole job through the C ABI: the edge list from pinned host memory "
                         "(CSR build included), felog_run to the stop-all rule, syn0 back to pinned host memory"},
+        "walks": walks,
         "gpu_launches": int(launches),
         "autotune": f.tuning_report(),
         "clocks": clk.summary(),
