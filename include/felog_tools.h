@@ -76,6 +76,18 @@ int felog_synth_write_graph(const felog_synth *s, const char *path);
 void felog_synth_free(felog_synth *s);
 
 /* Exact Mann-Whitney AUC in FP64 (ties count 1/2). Returns NaN when a class is empty. */
+/* The held-out split of the reference's gtrain tool (src/tools/gtrain.cpp:293-343)
+ * over n undirected edges: floor(holdout * n) positives (float arithmetic,
+ * like the tool's float -s), each drawn by swap-to-tail until both endpoints
+ * keep degree >= 1, and as many negatives (pairs that are no edge, distinct as
+ * ordered pairs, self pairs allowed, as in the tool), every draw from one
+ * 31-bit stream keyed by seed in the tool's order (its rand() calls through
+ * get_big_rand).  train: n entries (the kept edges in the tool's swapped
+ * order, *n_train of them); test_*: 2 * floor(holdout * n) entries, positives
+ * first.  Returns 0, -1 on bad arguments, -3 when a draw loop runs away. */
+int felog_heldout_split(const felog_edge12 *edges, uint64_t n, uint32_t v_num, double holdout, uint64_t seed,
+                        felog_edge12 *train, uint64_t *n_train, uint32_t *test_src, uint32_t *test_dst,
+                        uint8_t *test_label, uint64_t *n_test);
 double felog_auc(const float *scores, const uint8_t *labels, size_t n);
 
 /* Reads a 12-byte binary edge file (storage.hpp:40-61 semantics: whole records only).

@@ -38,6 +38,86 @@ struct Cand {
 
 }  // namespace
 
+// 31-bit values of the split's random stream: value k of stream (seed ^ 0x5117, 1),
+// in [0, 2^31 - 1], as rand() gives them to gtrain.cpp's get_big_rand.
+inline uint64_t split_rand(uint64_t seed, uint64_t k) { return draw(seed ^ 0x5117ULL, 1, k) >> 33; }
+
+// get_big_rand (gtrain.cpp:214-223) on the split stream; RAND_MAX = 2^31 - 1
+inline uint64_t split_big_rand(uint64_t seed, uint64_t &k, uint64_t range) {
+  const uint64_t rmax = 2147483647ULL;
+  if (range < rmax) return split_rand(seed, k++) % range;
+  const uint64_t round = range / rmax, mod = range % rmax;
+  const uint64_t t = split_rand(seed, k++) % round + 1;
+  if (t == round) return t * rmax + split_rand(seed, k++) % mod;
+  return t * rmax + split_rand(seed, k++) % rmax;
+}
+
+// The held-out split of gtrain.cpp:293-343 over edges (in place): npos =
+// holdout * E (float arithmetic, as the tool's float sample); positives by
+// swap-to-tail, each drawn until both endpoints still have degree > 1, which
+// then drops by one; negatives as (src, dst) draws until the pair is no
+// edge and src -> dst is not yet a negative (a pair and its reverse are two
+// candidates, a vertex paired with itself is allowed, as in the tool).  One
+// random stream feeds every draw in the tool's order.  The train edges are
+// edges[0 .. E - npos).  Returns npos, or ~0 when a draw loop runs away.
+static uint64_t heldout_split(std::vector<felog_edge12> &edges, uint32_t nv, double holdout, uint64_t seed,
+                       std::vector<uint32_t> &tsrc, std::vector<uint32_t> &tdst, std::vector<uint8_t> &tlab) {
+  const uint64_t E = edges.size();
+  const uint64_t npos = (uint64_t)((float)holdout * (float)E);
+  std::vector<uint64_t> deg(nv, 0);
+  for (auto &e : edges) {
+    deg[e.src]++;
+    deg[e.dst]++;
+  }
+  tsrc.clear();
+  tdst.clear();
+  tlab.clear();
+  tsrc.reserve(2 * npos);
+  tdst.reserve(2 * npos);
+  tlab.reserve(2 * npos);
+  if (npos > E) return ~0ULL;
+  uint64_t k = 0, tail = E - 1;
+  std::vector<uint64_t> pos_src, pos_dst;
+  for (uint64_t i = 0; i < npos; i++) {
+    uint64_t ep, guard = 0;
+    do {
+      ep = split_big_rand(seed, k, tail + 1);
+      if (++guard > 1000000000ULL) return ~0ULL;
+    } while (deg[edges[ep].src] <= 1 || deg[edges[ep].dst] <= 1);
+    tsrc.push_back(edges[ep].src);
+    tdst.push_back(edges[ep].dst);
+    tlab.push_back(1);
+    deg[edges[ep].src]--;
+    deg[edges[ep].dst]--;
+    std::swap(edges[ep], edges[tail]);
+    tail--;
+  }
+  std::unordered_set<uint64_t> edge_set;
+  edge_set.reserve(E * 2);
+  for (auto &e : edges) {
+    uint64_t lo = std::min(e.src, e.dst), hi = std::max(e.src, e.dst);
+    edge_set.insert((lo << 32) | hi);
+  }
+  std::unordered_set<uint64_t> neg_set;  // directed: src << 32 | dst
+  neg_set.reserve(npos * 2 + 1);
+  for (uint64_t i = 0; i < npos; i++) {
+    uint64_t guard = 0;
+    for (;;) {
+      const uint32_t a = (uint32_t)split_big_rand(seed, k, nv);
+      const uint32_t b = (uint32_t)split_big_rand(seed, k, nv);
+      if (++guard > 1000000000ULL) return ~0ULL;
+      const uint64_t lo = std::min(a, b), hi = std::max(a, b);
+      if (a != b && edge_set.count((lo << 32) | hi)) continue;
+      if (!neg_set.insert(((uint64_t)a << 32) | b).second) continue;
+      tsrc.push_back(a);
+      tdst.push_back(b);
+      tlab.push_back(0);
+      break;
+    }
+  }
+  return npos;
+}
+
 struct felog_synth {
   felog_synth_info info;
   std::vector<felog_edge12> train;
@@ -155,56 +235,16 @@ extern "C" int felog_synth_generate(const felog_synth_params *p, felog_synth **o
     deg[e.dst]++;
   }
 
-  // ---- held-out positives: gtrain.cpp:293-327 (swap-to-tail) ----
-  uint64_t npos = (uint64_t)(p->holdout * (double)E);
+  // ---- the held-out split (gtrain.cpp:293-343), see felog_heldout_split ----
   std::vector<uint32_t> tsrc, tdst;
   std::vector<uint8_t> tlab;
-  tsrc.reserve(2 * npos);
-  tdst.reserve(2 * npos);
-  tlab.reserve(2 * npos);
-  uint64_t tail = E - 1;
-  uint64_t ctr = 0;
-  for (uint64_t k = 0; k < npos; k++) {
-    uint64_t ep;
-    uint64_t guard = 0;
-    do {
-      ep = draw(p->seed ^ 0x5117ULL, 1, ctr++) % (tail + 1);
-      if (++guard > 1000000000ULL) { delete s; return -3; }
-    } while (deg[edges[ep].src] <= 1 || deg[edges[ep].dst] <= 1);
-    tsrc.push_back(edges[ep].src);
-    tdst.push_back(edges[ep].dst);
-    tlab.push_back(1);
-    deg[edges[ep].src]--;
-    deg[edges[ep].dst]--;
-    std::swap(edges[ep], edges[tail]);
-    tail--;
+  uint64_t npos = heldout_split(edges, nv, p->holdout, p->seed, tsrc, tdst, tlab);
+  if (npos == ~0ULL) { delete s; return -3; }
+  {
+    std::vector<uint64_t> d2(nv, 0);
+    for (uint64_t i = 0; i < E - npos; i++) { d2[edges[i].src]++; d2[edges[i].dst]++; }
+    deg.swap(d2);
   }
-  // ---- negatives: gtrain.cpp:329-343 (random non-edges, no repeats) ----
-  std::unordered_set<uint64_t> edge_set;
-  edge_set.reserve(E * 2);
-  for (auto &e : edges) {
-    uint64_t lo = std::min(e.src, e.dst), hi = std::max(e.src, e.dst);
-    edge_set.insert((lo << 32) | hi);
-  }
-  std::unordered_set<uint64_t> neg_set;
-  neg_set.reserve(npos * 2 + 1);
-  for (uint64_t k = 0; k < npos; k++) {
-    uint64_t guard = 0;
-    for (;;) {
-      uint32_t a = (uint32_t)(draw(p->seed ^ 0x4E47ULL, 2, ctr++) % nv);
-      uint32_t b = (uint32_t)(draw(p->seed ^ 0x4E47ULL, 2, ctr++) % nv);
-      if (++guard > 1000000000ULL) { delete s; return -3; }
-      if (a == b) continue;
-      uint64_t lo = std::min(a, b), hi = std::max(a, b), key = (lo << 32) | hi;
-      if (edge_set.count(key) || neg_set.count(key)) continue;
-      neg_set.insert(key);
-      tsrc.push_back(a);
-      tdst.push_back(b);
-      tlab.push_back(0);
-      break;
-    }
-  }
-
   edges.resize(E - npos);
   uint64_t maxd = 0;
   for (uint32_t v = 0; v < nv; v++) maxd = std::max(maxd, deg[v]);
@@ -295,4 +335,27 @@ extern "C" double felog_auc(const float *scores, const uint8_t *labels, size_t n
   }
   double u = rank_sum - (double)npos * (double)(npos + 1) / 2.0;
   return u / ((double)npos * (double)nneg);
+}
+
+extern "C" int felog_heldout_split(const felog_edge12 *edges, uint64_t n, uint32_t v_num, double holdout,
+                                   uint64_t seed, felog_edge12 *train, uint64_t *n_train, uint32_t *test_src,
+                                   uint32_t *test_dst, uint8_t *test_label, uint64_t *n_test) {
+  if ((n && (!edges || !train)) || !n_train || !n_test || holdout < 0.0 || holdout >= 1.0) return -1;
+  for (uint64_t i = 0; i < n; i++)
+    if (edges[i].src >= v_num || edges[i].dst >= v_num) return -1;
+  std::vector<felog_edge12> e(edges, edges + n);
+  std::vector<uint32_t> ts, td;
+  std::vector<uint8_t> tl;
+  const uint64_t npos = heldout_split(e, v_num, holdout, seed, ts, td, tl);
+  if (npos == ~0ULL) return -3;
+  if (ts.size() && (!test_src || !test_dst || !test_label)) return -1;
+  *n_train = n - npos;
+  *n_test = ts.size();
+  if (*n_train) memcpy(train, e.data(), sizeof(felog_edge12) * *n_train);
+  if (*n_test) {
+    memcpy(test_src, ts.data(), 4 * ts.size());
+    memcpy(test_dst, td.data(), 4 * td.size());
+    memcpy(test_label, tl.data(), tl.size());
+  }
+  return 0;
 }

@@ -208,6 +208,8 @@ def tools_lib():
         L.felog_synth_free.argtypes = [_P]
         L.felog_synth_free.restype = None
         L.felog_auc.argtypes = [_P, _P, ctypes.c_size_t]
+        L.felog_heldout_split.argtypes = [_P, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_double, ctypes.c_uint64, _P,
+                                          _P, _P, _P, _P, _P]
         L.felog_auc.restype = ctypes.c_double
         L.felog_read_edge_file.argtypes = [ctypes.c_char_p, _P, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]
         L.felog_write_edge_file.argtypes = [ctypes.c_char_p, _P, ctypes.c_size_t]
@@ -609,6 +611,22 @@ def build_alias_noalloc(row_ptr_dev, weight_dev, v_num, e_num, prob_dev, alias_d
     st = L.felog_build_alias_noalloc(row_ptr_dev, weight_dev, v_num, e_num, prob_dev, alias_dev, stream)
     if st != 0:
         raise FelogError(st, "felog_build_alias_noalloc failed (oversized graph, bad weight or CUDA error)")
+
+
+def heldout_split(edges, v_num, holdout, seed):
+    """felog_heldout_split (the gtrain tool's split): returns (train edges, test_src, test_dst, test_label)."""
+    L = tools_lib()
+    e = np.ascontiguousarray(edges, dtype=EDGE12)
+    n = len(e)
+    train = np.zeros(max(n, 1), EDGE12)
+    cap = 2 * n + 2
+    ts, td, tl = np.zeros(cap, np.uint32), np.zeros(cap, np.uint32), np.zeros(cap, np.uint8)
+    nt, nx = ctypes.c_uint64(), ctypes.c_uint64()
+    rc = L.felog_heldout_split(_addr(e), n, v_num, holdout, seed, _addr(train), ctypes.byref(nt), _addr(ts),
+                               _addr(td), _addr(tl), ctypes.byref(nx))
+    if rc != 0:
+        raise FelogError(1, f"felog_heldout_split failed ({rc})")
+    return train[: nt.value], ts[: nx.value], td[: nx.value], tl[: nx.value]
 
 
 def auc(scores, labels):

@@ -7,6 +7,10 @@ reference's own output on seeded synthetic inputs:
 
   walk_*.npz   include/walk.hpp run by oracle/_ref/ref_walk with injected draws:
                the graph, per-walker draw streams and the per-round corpus.
+  split_*.npz  src/tools/gtrain.cpp (the held-out split tool) run by
+               oracle/_ref/ref_gtrain with its rand() fed from the split's
+               seeded stream: the input edges and the tool's train edges,
+               test pairs and labels.
   gcn_*.npz    src/tools/gcn.cpp (the offline common-neighbour tool) run by
                oracle/_ref/ref_gcn on text edge lists: per input edge its
                common-neighbour count.
@@ -16,7 +20,7 @@ reference's own output on seeded synthetic inputs:
                thresholds, unigram table digest, syn0 head and the batch plan
                (sentence_length, sen, negSample per batch).
 
-Usage: python tests/golden/make_fixtures.py [walk] [plan] [gcn]   (default: all)
+Usage: python tests/golden/make_fixtures.py [walk] [plan] [gcn] [split]   (default: all)
 """
 import hashlib
 import os
@@ -223,8 +227,41 @@ def gcn_fixtures():
     run_gcn_fixture("gcn_rmat4096_undirected.npz", src, dst, g["v_num"], True)
 
 
+def run_split_fixture(name, edges, V, sample, seed):
+    with tempfile.TemporaryDirectory() as td:
+        paths = [os.path.join(td, x) for x in ("e.txt", "tr.txt", "te.txt", "tl.txt")]
+        with open(paths[0], "w") as fh:
+            fh.write("".join(f"{a}\t{b}\t0\n" for a, b in zip(edges["src"].tolist(), edges["dst"].tolist())))
+        subprocess.run([os.path.join(REFBIN, "ref_gtrain")] + paths + [repr(sample), str(V), str(seed)], check=True,
+                       stdout=subprocess.DEVNULL)
+        tr = np.loadtxt(paths[1], dtype=np.uint32, ndmin=2)
+        te = np.loadtxt(paths[2], dtype=np.uint32, ndmin=2)
+        tl = np.loadtxt(paths[3], dtype=np.uint8, ndmin=1)
+    np.savez_compressed(os.path.join(HERE, name), src=edges["src"], dst=edges["dst"], v_num=np.uint32(V),
+                        sample=np.float64(sample), seed=np.uint64(seed), train_src=tr[:, 0], train_dst=tr[:, 1],
+                        test_src=te[:, 0], test_dst=te[:, 1], test_label=tl)
+    print(name, len(edges), "edges ->", len(tr), "train,", len(tl), "test", flush=True)
+
+
+def split_fixtures():
+    g = fb.synth_graph(seed=5, v_target=300, e_target=1200, holdout=0.0)
+    run_split_fixture("split_rmat300.npz", g["edges"], g["v_num"], 0.1, 77)
+    g = fb.synth_graph(seed=6, v_target=4096, e_target=30000, holdout=0.0)
+    run_split_fixture("split_rmat4096.npz", g["edges"], g["v_num"], 0.05, 78)
+    # a star and a path: many degree-1 endpoints (redrawn positives), few non-edges per vertex
+    star = np.zeros(60, fb.EDGE12)
+    star["src"] = 0
+    star["dst"] = np.arange(1, 61)
+    path = np.zeros(59, fb.EDGE12)
+    path["src"] = np.arange(1, 60)
+    path["dst"] = np.arange(2, 61)
+    run_split_fixture("split_star_path.npz", np.concatenate([star, path]), 61, 0.2, 79)
+
+
 def main():
-    parts = set(sys.argv[1:]) or {"walk", "plan", "gcn"}
+    parts = set(sys.argv[1:]) or {"walk", "plan", "gcn", "split"}
+    if "split" in parts:
+        split_fixtures()
     if "gcn" in parts:
         gcn_fixtures()
     if "walk" not in parts and "plan" not in parts:

@@ -68,7 +68,10 @@ def test_synth_graph_contract():
     assert lab[:npos].all() and not lab[npos:].any() and len(lab) == 2 * npos
     neg = np.minimum(g["test_src"][npos:], g["test_dst"][npos:]).astype(np.uint64) << 32 | \
         np.maximum(g["test_src"][npos:], g["test_dst"][npos:])
-    assert not np.isin(neg, key).any() and len(np.unique(neg)) == npos
+    # negatives are no edges and distinct as ordered pairs (gtrain.cpp:329-343 keeps a pair and its
+    # reverse apart)
+    ordered = g["test_src"][npos:].astype(np.uint64) << 32 | g["test_dst"][npos:]
+    assert not np.isin(neg, key).any() and len(np.unique(ordered)) == npos
     # deterministic in the seed
     g2 = fb.synth_graph(seed=4, v_target=2048, e_target=8192, holdout=0.1)
     assert np.array_equal(g2["edges"], e)
