@@ -369,6 +369,17 @@ def bench_mine(args):
             job(cnt, timed=True)
     ms = cnt["ms"]
     launches = f.kernel_launches() - launches0
+    lost = None
+    if prec == "bf16" and FORMS[form]["reuse_neg"] == 0:
+        # one more job with the lost-update count on (outside the timed region)
+        f.init_model()
+        f.count_lost_updates(True)
+        rs_l = f.run()
+        nu, nl = f.lost_updates()
+        f.count_lost_updates(False)
+        lost = {"bf16_row_updates": nu, "overwritten": nl, "share": nl / max(nu, 1), "rounds": rs_l["rounds"],
+                "what": "BF16-row stores of one job that overwrote another warp's concurrent update of the row "
+                        "(Hogwild plain stores; FP32 master rows add atomically)"}
     # the walker against the attainable rate of its own access pattern: the
     # memory skeleton of the last round (same walkers and lengths, dependent
     # uniform-neighbour gathers, no arithmetic), timed outside the timed region
@@ -488,6 +499,7 @@ def bench_mine(args):
                 "what": "per step one whole job through the C ABI: the edge list from pinned host memory "
                         "(CSR build included), felog_run to the stop-all rule, syn0 back to pinned host memory"},
         "walks": walks,
+        "bf16_lost_updates": lost,
         "gpu_launches": int(launches),
         "autotune": f.tuning_report(),
         "clocks": clk.summary(),

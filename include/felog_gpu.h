@@ -107,6 +107,8 @@ typedef struct felog_opts {
   int32_t autotune;         /* 1 (default): the first round picks the pair trainer's launch shape by timing */
   uint32_t stream_walkers;  /* felog_run: walk and train each round in pieces of this many walkers, so the
                                corpus of a whole round is never resident (0: whole rounds) */
+  int32_t bf16_reread;      /* BF16 form: read a row again right before its store, so concurrent updates of
+                               it are kept (0: for vocabularies below 2^20 rows, 1 always, -1 never) */
 } felog_opts;
 
 typedef struct felog_ctx felog_ctx;
@@ -333,6 +335,16 @@ felog_status felog_wait_embeddings(felog_ctx *ctx);
 felog_status felog_score_pairs(felog_ctx *ctx, const int32_t *ctx_rows, const int32_t *tgt_rows,
                                const int8_t *labels, const uint64_t *batch_of, uint64_t n, uint64_t n_batches,
                                float *dots, double *batch_loss);
+/* No counterpart in the reference (diagnostic of the BF16 form).  BF16 rows are
+ * written back with plain stores (Hogwild), so two warps that update one row
+ * at the same time can overwrite each other.  With counting on, the pair
+ * trainer keeps a store version per row: a store finding its row's version
+ * moved since its warp read the row has overwritten another warp's update.
+ * felog_lost_updates: BF16-row updates and overwritten ones since counting
+ * was turned on (FP32 master rows add atomically and lose nothing).  Same
+ * training otherwise; counting costs an atomic per BF16-row store. */
+felog_status felog_count_lost_updates(felog_ctx *ctx, int on);
+felog_status felog_lost_updates(felog_ctx *ctx, uint64_t *bf16_updates, uint64_t *lost);
 /* the batch plan of the last felog_train_round (parity checks) */
 felog_status felog_plan_size(felog_ctx *ctx, uint64_t *n_sentences, uint64_t *n_sen, uint64_t *n_batches);
 felog_status felog_get_plan(felog_ctx *ctx, int32_t *sen, uint64_t *sent_start, uint64_t *batch_first,

@@ -151,6 +151,9 @@ struct felog_ctx {
   DevBuf<uint64_t> pr_count, pr_off;  // pair stream: pairs per sentence, offsets
   DevBuf<int32_t> pr_rec;             // pair stream records
   int pair_minb = 0;                  // autotuned blocks per SM of the pair trainer (0: not tuned yet)
+  bool count_lost = false;            // BF16 pair trainer counts overwritten row updates (diagnostic)
+  DevBuf<uint32_t> lost_ver0, lost_ver1;
+  DevBuf<unsigned long long> lost_tot;
   std::string tuning;                 // what the autotuner measured and chose
   DevBuf<unsigned long long> pr_cstate, pr_jump;
   DevBuf<uint32_t> pr_cfirst;
@@ -1582,6 +1585,16 @@ void launch_trainer(felog_ctx *c, const SgArgs &g, int blocks, int threads) {
 
 template <int D, int K, class P>
 void launch_pairs_dkp(felog_ctx *c, const SgArgs &g, int blocks, int threads, uint64_t base, uint64_t s0) {
+  if constexpr (P::kBF16 && D <= 128) {
+    if (c->count_lost) {  // diagnostic variant: same training, plus the lost-update count
+      SgArgs gc = g;
+      gc.ver0 = c->lost_ver0.p;
+      gc.ver1 = c->lost_ver1.p;
+      gc.lost = c->lost_tot.p;
+      k_sgns_train_pairs<D, K, P, 5, true><<<blocks, threads, 0, c->stream>>>(gc, c->pr_rec.p, c->pr_off.p, base, s0);
+      return;
+    }
+  }
   // untuned: 5 blocks per SM for BF16 rows (48 registers), 4 for FP32 rows (5 spills)
   const int minb = D >= 256 ? 2 : (c->pair_minb ? c->pair_minb : (P::kBF16 ? 5 : 4));
   if (minb == 2) k_sgns_train_pairs<D, K, P, 2><<<blocks, threads, 0, c->stream>>>(g, c->pr_rec.p, c->pr_off.p, base, s0);
@@ -1817,6 +1830,10 @@ extern "C" felog_status felog_train_round(felog_ctx *c, uint32_t round, float al
   g.syn0_bf = c->syn0_bf.p;
   g.syn1_bf = c->syn1_bf.p;
   g.n_hot = c->n_f32;
+  // re-read before store: asked for, or automatic below 2^20 vocabulary rows, where
+  // thousands of warps share few rows and plain stores would overwrite most concurrent updates
+  g.reread = c->o.precision == FELOG_BF16 &&
+             (c->o.bf16_reread > 0 || (c->o.bf16_reread == 0 && c->vocab_size < (1ll << 20)));
   g.sr_seed = sr_hash((uint32_t)c->o.seed ^ sr_hash((uint32_t)(c->o.seed >> 32) + round * 0x9E3779B9u));
   // a streamed round trains its pieces one by one; each piece gets its own rounding seed
   if (c->chunk_base) g.sr_seed = sr_hash(g.sr_seed ^ sr_hash(c->chunk_base));
@@ -1894,6 +1911,39 @@ extern "C" felog_status felog_train_round(felog_ctx *c, uint32_t round, float al
     stats->ms_plan = ms_plan;
     stats->ms_train = ms_train;
   }
+  return FELOG_OK;
+}
+
+extern "C" felog_status felog_count_lost_updates(felog_ctx *c, int on) {
+  if (!c) return FELOG_INVALID_ARG;
+  if (!c->model_ready) return fail(c, FELOG_NOT_READY, "model not initialised");
+  CK(cudaSetDevice(c->device), "count_lost_updates");
+  c->count_lost = false;
+  c->lost_ver0.release();
+  c->lost_ver1.release();
+  c->lost_tot.release();
+  if (!on) return FELOG_OK;
+  if (c->o.precision != FELOG_BF16 || c->o.size > 128)
+    return fail(c, FELOG_INVALID_ARG, "count_lost_updates: the BF16 form of the pair trainer (-size <= 128) only");
+  const size_t n = (size_t)c->vocab_size;
+  CK(c->lost_ver0.ensure(n), "count_lost_updates");
+  CK(c->lost_ver1.ensure(n), "count_lost_updates");
+  CK(c->lost_tot.ensure(2), "count_lost_updates");
+  CK(cudaMemsetAsync(c->lost_ver0.p, 0, 4 * n, c->stream), "count_lost_updates");
+  CK(cudaMemsetAsync(c->lost_ver1.p, 0, 4 * n, c->stream), "count_lost_updates");
+  CK(cudaMemsetAsync(c->lost_tot.p, 0, 16, c->stream), "count_lost_updates");
+  CK(cudaStreamSynchronize(c->stream), "count_lost_updates");
+  c->count_lost = true;
+  return FELOG_OK;
+}
+
+extern "C" felog_status felog_lost_updates(felog_ctx *c, uint64_t *bf16_updates, uint64_t *lost) {
+  if (!c) return FELOG_INVALID_ARG;
+  if (!c->count_lost) return fail(c, FELOG_NOT_READY, "lost_updates: counting is off (felog_count_lost_updates)");
+  unsigned long long h[2];
+  RB(h, c->lost_tot.p, sizeof h, "lost_updates");
+  if (bf16_updates) *bf16_updates = h[0];
+  if (lost) *lost = h[1];
   return FELOG_OK;
 }
 

@@ -224,12 +224,14 @@ struct LaneRows {
   const float *f[2];     // FP32 rows of syn0 / syn1 with this lane's offset
   const uint16_t *b[2];  // BF16 rows with this lane's offset, shifted so row r is at b + r * DIM
   uint32_t n_hot;
+  bool reread;           // BF16 rows read again right before their store (SgArgs::reread)
 
   __device__ __forceinline__ void init(const SgArgs &a) {
     const int lo = lane_id() * J;
     f[0] = a.syn0 + lo;
     f[1] = a.syn1 + lo;
     n_hot = 0;
+    reread = a.reread != 0;
     b[0] = b[1] = nullptr;
     if constexpr (P::kBF16) {
       n_hot = (uint32_t)a.n_hot;
@@ -268,6 +270,12 @@ struct LaneRows {
       return false;
     } else {
       const bool hot = row < n_hot;
+      if (!hot && reread) {
+        uint32_t hv[H];
+        load_b16(b[W] + (size_t)row * DIM, hv);
+#pragma unroll
+        for (int k = 0; k < H; k++) cur[k] = make_float2(bf16_lo(hv[k]), bf16_hi(hv[k]));
+      }
       uint32_t w[H];
 #pragma unroll
       for (int k = 0; k < H; k++) {
@@ -322,6 +330,14 @@ struct LaneRows {
     }
   }
 };
+
+// lost-update count of one store to a BF16 row (lane 0 of the warp)
+__device__ __forceinline__ void count_store(uint32_t *ver, uint32_t row, uint32_t seen, uint32_t n_hot,
+                                            unsigned long long &n_cold, unsigned long long &n_lost) {
+  if (row < n_hot || lane_id() != 0) return;
+  n_cold++;
+  if (atomicAdd(&ver[row], 1u) != seen) n_lost++;
+}
 
 // in-lane part of the reference tree (pair t with t + DIM/2 via a*b + c, then
 // halve) on packed values; lane value j is element j % 2 of pair j / 2
@@ -392,7 +408,10 @@ __device__ __forceinline__ int rec_at(const int4 (&v)[S / 4], int i) {
 // sees the earlier update as in the reference.
 // MINB: resident 256-thread blocks per SM the register budget is built for
 // (the launch-shape autotuner picks among 2, 3, 4 and 5 for DIM <= 128).
-template <int DIM, int NK, class P, int MINB = (DIM >= 256 ? 2 : 4)>
+// CNT (diagnostic, BF16 rows): every cold-row store bumps the row's version;
+// a store whose row changed version since this warp read it overwrote another
+// warp's update, which is counted as lost.
+template <int DIM, int NK, class P, int MINB = (DIM >= 256 ? 2 : 4), bool CNT = false>
 __global__ void __launch_bounds__(256, MINB)
     k_sgns_train_pairs(SgArgs a, const int32_t *__restrict__ rec, const uint64_t *__restrict__ off, uint64_t base,
                        uint64_t s0) {
@@ -406,6 +425,7 @@ __global__ void __launch_bounds__(256, MINB)
   const int lane = lane_id();
   LaneRows<DIM, P> rows;
   rows.init(a);
+  unsigned long long n_cold = 0, n_lost = 0;  // CNT only
   unsigned long long sc;
   while (claim_sentence(a, sc)) {
     const uint64_t gs = s0 + sc;  // sentence index in the round's plan
@@ -430,6 +450,12 @@ __global__ void __launch_bounds__(256, MINB)
       for (int q = 0; q < NT; q++) tg[q] = rec_at<S>(cur, 1 + q);
       const bool dup = (r0 & kPairDup) != 0;
       float2 x[H];
+      uint32_t seen[NT + 1];
+      if constexpr (CNT) {
+        seen[NT] = __ldcg(&a.ver0[l1]);
+#pragma unroll
+        for (int q = 0; q < NT; q++) seen[q] = tg[q] >= 0 ? __ldcg(&a.ver1[tg[q]]) : 0u;
+      }
       rows.template load<0>(l1, x);
       float2 y[NT][H];
 #pragma unroll
@@ -456,7 +482,9 @@ __global__ void __launch_bounds__(256, MINB)
               neu[k] = __ffma2_rn(g2, y[q][k], neu[k]);
               upd[k] = __fmul2_rn(g2, x[k]);
             }
+            if constexpr (CNT) if (rows.reread) seen[q] = __ldcg(&a.ver1[tg[q]]);  // the window starts at the re-read
             rows.template update<1>((uint32_t)tg[q], upd, y[q], key, (uint32_t)q);
+            if constexpr (CNT) count_store(a.ver1, (uint32_t)tg[q], seen[q], rows.n_hot, n_cold, n_lost);
           }
           done = true;
         }
@@ -475,6 +503,11 @@ __global__ void __launch_bounds__(256, MINB)
             upd[k] = __fmul2_rn(g2, x[k]);
           }
           const bool stored = rows.template update<1>((uint32_t)tg[q], upd, y[q], key, (uint32_t)q);
+          if constexpr (CNT) {
+            count_store(a.ver1, (uint32_t)tg[q], seen[q], rows.n_hot, n_cold, n_lost);
+#pragma unroll
+            for (int r = q + 1; r < NT; r++) seen[r] += tg[r] == tg[q] ? 1u : 0u;  // this warp's own store
+          }
 #pragma unroll
           for (int r = q + 1; r < NT; r++)
             if (tg[r] == tg[q])
@@ -482,8 +515,14 @@ __global__ void __launch_bounds__(256, MINB)
               for (int k = 0; k < H; k++) y[r][k] = stored ? y[q][k] : __fadd2_rn(y[q][k], upd[k]);
         }
       }
+      if constexpr (CNT) if (rows.reread) seen[NT] = __ldcg(&a.ver0[l1]);
       rows.template update<0>(l1, neu, x, key, kSlotCtx);
+      if constexpr (CNT) count_store(a.ver0, l1, seen[NT], rows.n_hot, n_cold, n_lost);
     }
+  }
+  if constexpr (CNT) {
+    if (lane == 0 && n_cold) atomicAdd(&a.lost[0], n_cold);
+    if (lane == 0 && n_lost) atomicAdd(&a.lost[1], n_lost);
   }
 }
 

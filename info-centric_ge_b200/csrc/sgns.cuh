@@ -80,6 +80,13 @@ struct SgArgs {
   // the negative-draw LCG advanced by q + 1 steps: x -> lcg_a[q] x + lcg_c[q]
   unsigned long long lcg_a[kMaxNeg];
   unsigned long long lcg_c[kMaxNeg];
+  // lost-update count (diagnostic pair-trainer variant only): per-row store
+  // versions of syn0 / syn1 and the totals [cold-row updates, overwritten ones]
+  uint32_t *ver0, *ver1;
+  unsigned long long *lost;
+  // BF16 rows are read again right before their store, so a concurrent
+  // update lands in the stored value unless it falls in that last round trip
+  int reread;
 };
 
 // ------------------------------------------------------------ row access
@@ -211,6 +218,12 @@ __device__ __forceinline__ bool row_update(const SgArgs &a, int which, long long
   if constexpr (P::kBF16) {
     if (row >= a.n_hot) {
       constexpr int W = (J + 1) / 2;
+      if (a.reread) {
+        float now[J];
+        row_load<DIM, P>(a, which, row, now);
+#pragma unroll
+        for (int j = 0; j < J; j++) cur[j] = now[j];
+      }
       uint32_t w[W];
 #pragma unroll
       for (int k = 0; k < W; k++) {

@@ -45,6 +45,7 @@ class FelogOpts(ctypes.Structure):
         ("long_arena_tokens", ctypes.c_uint64), ("wait_limit", ctypes.c_uint64),
         ("hot_rows", ctypes.c_int64), ("budget_confidence", ctypes.c_float), ("budget_audit", ctypes.c_float),
         ("autotune", ctypes.c_int32), ("stream_walkers", ctypes.c_uint32),
+        ("bf16_reread", ctypes.c_int32),
     ]
 
 
@@ -167,6 +168,8 @@ def gpu_lib():
         L.felog_get_embeddings.argtypes = [_P, _P, _P, ctypes.c_uint64]
         L.felog_set_embeddings.argtypes = [_P, _P, _P]
         L.felog_plan_size.argtypes = [_P, _P, _P, _P]
+        L.felog_count_lost_updates.argtypes = [_P, ctypes.c_int]
+        L.felog_lost_updates.argtypes = [_P, _P, _P]
         L.felog_score_pairs.argtypes = [_P, _P, _P, _P, _P, ctypes.c_uint64, ctypes.c_uint64, _P, _P]
         L.felog_budget_features.argtypes = [_P, _P]
         L.felog_budget_labels.argtypes = [_P, _P, _P]
@@ -483,6 +486,15 @@ class Felog:
         l = np.zeros(n, np.float32)
         self._ck(self._L.felog_mlp_predict(self.h, _addr(c), _addr(cf), _addr(l)))
         return c, cf, l
+
+    def count_lost_updates(self, on=True):
+        self._ck(self._L.felog_count_lost_updates(self.h, int(on)))
+
+    def lost_updates(self):
+        """(BF16-row updates, overwritten ones) since counting was turned on."""
+        n, lost = ctypes.c_uint64(), ctypes.c_uint64()
+        self._ck(self._L.felog_lost_updates(self.h, ctypes.byref(n), ctypes.byref(lost)))
+        return n.value, lost.value
 
     def plan(self):
         ns, nsen, nb = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()

@@ -64,3 +64,37 @@ extern "C" int ref_sgns_run_sentencewise(int cbow_mode, int dim, int win, int ne
   cudaFree(dl);
   return cudaGetLastError() == cudaSuccess ? 0 : -4;
 }
+
+/* The reference's convergence similarity kernel, batch_similarity_direct_index_optimized_kernel
+ * (word2vec.cu:1448-1506), launched as batch_node_neighbor_direct_index launches it
+ * (word2vec.cu:1833-1842: one block per pair, 128 threads, 256 beyond 200 dims) on
+ * given (node, neighbour) vertex pairs of a syn0 table in vocabulary order.
+ * out[i]: the cosine of pair i.  Returns 0, or a negative CUDA failure. */
+extern "C" int ref_pair_similarity(const float *h_syn0, long long vsize, int dim, const uint32_t *h_node,
+                                   const uint32_t *h_nbr, int n, const uint32_t *h_id2offset, long long V,
+                                   float *h_out) {
+  float *d0 = nullptr, *dr = nullptr;
+  vertex_id_t *dn = nullptr, *dm = nullptr, *di = nullptr;
+  size_t rows = (size_t)vsize * dim * sizeof(float);
+  if (cudaMalloc(&d0, rows) != cudaSuccess) return -1;
+  cudaMalloc(&dr, sizeof(float) * (size_t)(n > 0 ? n : 1));
+  cudaMalloc(&dn, sizeof(vertex_id_t) * (size_t)(n > 0 ? n : 1));
+  cudaMalloc(&dm, sizeof(vertex_id_t) * (size_t)(n > 0 ? n : 1));
+  cudaMalloc(&di, sizeof(vertex_id_t) * (size_t)V);
+  cudaMemcpy(d0, h_syn0, rows, cudaMemcpyHostToDevice);
+  cudaMemcpy(dn, h_node, sizeof(vertex_id_t) * n, cudaMemcpyHostToDevice);
+  cudaMemcpy(dm, h_nbr, sizeof(vertex_id_t) * n, cudaMemcpyHostToDevice);
+  cudaMemcpy(di, h_id2offset, sizeof(vertex_id_t) * V, cudaMemcpyHostToDevice);
+  int threads = dim > 200 ? 256 : 128;
+  if (n > 0)
+    batch_similarity_direct_index_optimized_kernel<<<n, threads, 3 * threads * sizeof(float)>>>(d0, dn, dm, dr, dim,
+                                                                                               n, di);
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e == cudaSuccess && n > 0) e = cudaMemcpy(h_out, dr, sizeof(float) * n, cudaMemcpyDeviceToHost);
+  cudaFree(d0);
+  cudaFree(dr);
+  cudaFree(dn);
+  cudaFree(dm);
+  cudaFree(di);
+  return e == cudaSuccess ? 0 : -2;
+}

@@ -341,6 +341,16 @@ def convergence(syn0, id2offset, dim, csr, stop_flags, seed, round_):
     return int(eva), sf, sim
 
 
+def eval_choose(seed, round_, v, deg):
+    """The convergence check's neighbour positions of vertex v (degree deg): all of
+    them in CSR order when deg <= 30, else the first 30 of the Philox shuffle."""
+    if deg <= 30:
+        return np.arange(deg, dtype=np.uint32)
+    out = np.zeros(30, np.uint32)
+    lib().orc_eval_choose(seed, round_, v, deg, ptr(out, u32p))
+    return out
+
+
 def round_kl(deg, freq):
     deg = np.ascontiguousarray(deg, np.uint32)
     freq = np.ascontiguousarray(freq, np.uint64)

@@ -36,7 +36,7 @@ def test_default_opts_follow_reference_defaults():
     assert abs(o.sample - 1e-3) < 1e-9 and abs(o.alpha - 0.025) < 1e-9
     assert (o.min_length, o.min_rounds, o.eval_batch_size) == (20, 5, 16384)
     # the Python mirror of felog_opts matches the C layout to its last field
-    assert ctypes.sizeof(fb.FelogOpts) == 160 and fb.FelogOpts.stream_walkers.offset == 156
+    assert ctypes.sizeof(fb.FelogOpts) == 168 and fb.FelogOpts.bf16_reread.offset == 160
     assert (o.seed, o.slot_len, o.hot_rows, o.autotune) == (0x5EED0001, 64, 0, 1)
     assert o.budget_confidence == 0.0 and o.budget_audit == 0.0
 

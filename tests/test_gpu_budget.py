@@ -125,3 +125,64 @@ def test_streamed_rounds_walk_the_same_corpus():
     assert a["rounds"] == b["rounds"] == 2
     assert a["walk_tokens"] == b["walk_tokens"] and a["train_words"] == b["train_words"]
     assert qa > 0.7 and abs(qa - qb) < 0.02, (qa, qb)
+
+
+def test_convergence_cosines_match_the_reference_kernel():
+    """k_converge's per-vertex mean cosine against the reference's own kernel:
+    batch_similarity_direct_index_optimized_kernel (word2vec.cu:1448-1506),
+    compiled from its source (oracle/_ref/libref_sgns_gpu.so) and launched as
+    batch_node_neighbor_direct_index launches it, on the same neighbour choices
+    (all neighbours up to 30, else the first 30 of the Philox shuffle), then
+    averaged per vertex as its host code does (FP32 sum in neighbour order,
+    divided by the count; word2vec.cu:1860-1876).  Bit for bit."""
+    import ctypes
+    import os
+
+    from conftest import ROOT
+
+    so = os.path.join(ROOT, "oracle", "_ref", "libref_sgns_gpu.so")
+    if not os.path.exists(so):
+        pytest.skip("reference harness not built (make -C oracle ref)")
+    L = ctypes.CDLL(so)
+    L.ref_pair_similarity.argtypes = [ctypes.c_void_p, ctypes.c_longlong, ctypes.c_int, ctypes.c_void_p,
+                                      ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_longlong,
+                                      ctypes.c_void_p]
+    fx = load_golden("walk_rmat4096.npz")
+    e, V = fx["edges"], int(fx["V"])
+    f = fb.Felog(v_num=V, size=128, window=10, negative=5, cbow=0, reuse_neg=0, min_count=0, seed=31)
+    f.load_graph(e, V)
+    f.init_model()
+    for r in range(2):
+        f.walk_round(r)
+        f.train_round(r)
+    s0, _ = f.embeddings()
+    _, id2, vs, _ = f.vocab()
+    f.set_stop_flags(np.zeros(V, np.uint8))
+    f.budget_check(1)
+    sim = f.similarity()
+    c = ob.OracleCsr(e, V)
+    node, nbr, cnt = [], [], np.zeros(V, np.int64)
+    for v in range(V):
+        b, d = int(c.row_ptr[v]), int(c.row_ptr[v + 1] - c.row_ptr[v])
+        ch = ob.eval_choose(f.opts.seed, 1, v, d)
+        node.extend([v] * len(ch))
+        nbr.extend(c.nbr[b + ch.astype(np.int64)].tolist())
+        cnt[v] = len(ch)
+    node = np.array(node, np.uint32)
+    nbr = np.array(nbr, np.uint32)
+    cos = np.zeros(len(node), np.float32)
+    s0c = np.ascontiguousarray(s0, np.float32)
+    id2c = np.ascontiguousarray(id2, np.uint32)
+    assert L.ref_pair_similarity(s0c.ctypes.data, vs, 128, node.ctypes.data, nbr.ctypes.data, len(node),
+                                 id2c.ctypes.data, V, cos.ctypes.data) == 0
+    ref = np.zeros(V, np.float32)
+    o = 0
+    for v in range(V):
+        acc = np.float32(0.0)
+        for j in range(cnt[v]):
+            acc = np.float32(acc + cos[o + j])
+        o += cnt[v]
+        ref[v] = acc / np.float32(cnt[v]) if cnt[v] else np.float32(0.0)
+    np.testing.assert_array_equal(sim, ref)
+    np.testing.assert_array_equal(f.stop_flags(), (ref > 0.65).astype(np.uint8))
+    f.close()

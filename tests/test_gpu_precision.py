@@ -270,3 +270,37 @@ def test_precision_study_1024_batches():
           f"mean {rl16.mean():.3e}; |f64| mean {np.abs(d64).mean():.3e}")
     assert rl32.max() < 1e-5
     assert rl16.max() < 1e-2
+
+
+def test_lost_update_count():
+    """felog_count_lost_updates: one warp in sentence order never overwrites a
+    concurrent update (0 lost, and the trained tables equal an uncounted run's);
+    Hogwild over many warps does, the more the fewer rows there are (this
+    8k-vertex graph is trained by thousands of warps at once), and the count is
+    reported."""
+    g = fb.synth_graph(seed=12, v_target=8192, e_target=65536, holdout=0.0)
+    V = g["v_num"]
+    res = {}
+    for det in (1, 0):
+        for count in (False, True):
+            f = fb.Felog(v_num=V, size=128, window=10, negative=5, cbow=0, reuse_neg=0, min_count=0, seed=3,
+                         precision=1, deterministic=det)
+            f.load_graph(g["edges"], V)
+            f.init_model()
+            if count:
+                f.count_lost_updates(True)
+            f.walk_round(0)
+            if det:
+                tok, off = f.corpus()
+                n = int(np.searchsorted(off, 20000))
+                f.set_corpus(tok[: int(off[n])], off[: n + 1])
+            f.train_round(0)
+            res[(det, count)] = (f.embeddings(), f.lost_updates() if count else None)
+            f.close()
+    (d0, _), (d1, (nu, nl)) = res[(1, False)], res[(1, True)]
+    assert nu > 0 and nl == 0
+    for a, b in zip(d0, d1):
+        np.testing.assert_array_equal(a, b)
+    nu, nl = res[(0, True)][1]
+    print(f"Hogwild: {nl} of {nu} BF16-row updates overwritten")
+    assert nu > 0 and 0 < nl <= nu
