@@ -108,7 +108,7 @@ typedef struct felog_opts {
   uint32_t stream_walkers;  /* felog_run: walk and train each round in pieces of this many walkers, so the
                                corpus of a whole round is never resident (0: whole rounds) */
   int32_t bf16_reread;      /* BF16 form: read a row again right before its store, so concurrent updates of
-                               it are kept (0: for vocabularies below 2^20 rows, 1 always, -1 never) */
+                               it are kept (0: for vocabularies below 2^17 rows, 1 always, -1 never) */
 } felog_opts;
 
 typedef struct felog_ctx felog_ctx;

@@ -1830,10 +1830,10 @@ extern "C" felog_status felog_train_round(felog_ctx *c, uint32_t round, float al
   g.syn0_bf = c->syn0_bf.p;
   g.syn1_bf = c->syn1_bf.p;
   g.n_hot = c->n_f32;
-  // re-read before store: asked for, or automatic below 2^20 vocabulary rows, where
+  // re-read before store: asked for, or automatic below 2^17 vocabulary rows, where
   // thousands of warps share few rows and plain stores would overwrite most concurrent updates
   g.reread = c->o.precision == FELOG_BF16 &&
-             (c->o.bf16_reread > 0 || (c->o.bf16_reread == 0 && c->vocab_size < (1ll << 20)));
+             (c->o.bf16_reread > 0 || (c->o.bf16_reread == 0 && c->vocab_size < (1ll << 17)));
   g.sr_seed = sr_hash((uint32_t)c->o.seed ^ sr_hash((uint32_t)(c->o.seed >> 32) + round * 0x9E3779B9u));
   // a streamed round trains its pieces one by one; each piece gets its own rounding seed
   if (c->chunk_base) g.sr_seed = sr_hash(g.sr_seed ^ sr_hash(c->chunk_base));
