@@ -1583,30 +1583,45 @@ void launch_trainer(felog_ctx *c, const SgArgs &g, int blocks, int threads) {
   }
 }
 
+template <int D, int K, class P, bool RR>
+void launch_pairs_minb(felog_ctx *c, const SgArgs &g, int blocks, int threads, uint64_t base, uint64_t s0) {
+  // untuned: 5 blocks per SM for BF16 rows (48 registers), 4 for FP32 rows (5 spills)
+  const int minb = D >= 256 ? 2 : (c->pair_minb ? c->pair_minb : (P::kBF16 ? 5 : 4));
+  constexpr int M2 = 2, M3 = D >= 256 ? 2 : 3, M4 = D >= 256 ? 2 : 4, M5 = D >= 256 ? 2 : 5;
+  if (minb == 2)
+    k_sgns_train_pairs<D, K, P, M2, RR><<<blocks, threads, 0, c->stream>>>(g, c->pr_rec.p, c->pr_off.p, base, s0);
+  else if (minb == 3)
+    k_sgns_train_pairs<D, K, P, M3, RR><<<blocks, threads, 0, c->stream>>>(g, c->pr_rec.p, c->pr_off.p, base, s0);
+  else if (minb == 5)
+    k_sgns_train_pairs<D, K, P, M5, RR><<<blocks, threads, 0, c->stream>>>(g, c->pr_rec.p, c->pr_off.p, base, s0);
+  else
+    k_sgns_train_pairs<D, K, P, M4, RR><<<blocks, threads, 0, c->stream>>>(g, c->pr_rec.p, c->pr_off.p, base, s0);
+}
+
 template <int D, int K, class P>
 void launch_pairs_dkp(felog_ctx *c, const SgArgs &g, int blocks, int threads, uint64_t base, uint64_t s0) {
-  if constexpr (P::kBF16 && D <= 128) {
-    if (c->count_lost) {  // diagnostic variant: same training, plus the lost-update count
-      SgArgs gc = g;
-      gc.ver0 = c->lost_ver0.p;
-      gc.ver1 = c->lost_ver1.p;
-      gc.lost = c->lost_tot.p;
-      k_sgns_train_pairs<D, K, P, 5, true><<<blocks, threads, 0, c->stream>>>(gc, c->pr_rec.p, c->pr_off.p, base, s0);
+  if constexpr (P::kBF16) {
+    if constexpr (D <= 128) {
+      if (c->count_lost) {  // diagnostic variant: same training, plus the lost-update count
+        SgArgs gc = g;
+        gc.ver0 = c->lost_ver0.p;
+        gc.ver1 = c->lost_ver1.p;
+        gc.lost = c->lost_tot.p;
+        if (g.reread)
+          k_sgns_train_pairs<D, K, P, 5, true, true><<<blocks, threads, 0, c->stream>>>(gc, c->pr_rec.p, c->pr_off.p,
+                                                                                       base, s0);
+        else
+          k_sgns_train_pairs<D, K, P, 5, false, true><<<blocks, threads, 0, c->stream>>>(gc, c->pr_rec.p, c->pr_off.p,
+                                                                                        base, s0);
+        return;
+      }
+    }
+    if (g.reread) {
+      launch_pairs_minb<D, K, P, true>(c, g, blocks, threads, base, s0);
       return;
     }
   }
-  // untuned: 5 blocks per SM for BF16 rows (48 registers), 4 for FP32 rows (5 spills)
-  const int minb = D >= 256 ? 2 : (c->pair_minb ? c->pair_minb : (P::kBF16 ? 5 : 4));
-  if (minb == 2) k_sgns_train_pairs<D, K, P, 2><<<blocks, threads, 0, c->stream>>>(g, c->pr_rec.p, c->pr_off.p, base, s0);
-  else if (minb == 3)
-    k_sgns_train_pairs<D, K, P, (D >= 256 ? 2 : 3)><<<blocks, threads, 0, c->stream>>>(g, c->pr_rec.p, c->pr_off.p, base,
-                                                                                      s0);
-  else if (minb == 5)
-    k_sgns_train_pairs<D, K, P, (D >= 256 ? 2 : 5)><<<blocks, threads, 0, c->stream>>>(g, c->pr_rec.p, c->pr_off.p, base,
-                                                                                      s0);
-  else
-    k_sgns_train_pairs<D, K, P, (D >= 256 ? 2 : 4)><<<blocks, threads, 0, c->stream>>>(g, c->pr_rec.p, c->pr_off.p, base,
-                                                                                      s0);
+  launch_pairs_minb<D, K, P, false>(c, g, blocks, threads, base, s0);
 }
 
 template <int K, class P>

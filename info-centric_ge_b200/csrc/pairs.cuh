@@ -216,22 +216,24 @@ __global__ void __launch_bounds__(256) k_pair_emit(PairArgs a) {
 // ---- row access for the pair trainer (DIM >= 64, J = DIM / 32 >= 2): each
 // lane's J values as J / 2 float2, so the elementwise work runs on the packed
 // FP32 pipe (one instruction per two values, each value rounded as in the
-// scalar form).
-template <int DIM, class P>
+// scalar form).  RR: read a BF16 row again right before its store (1), never
+// (0), or as SgArgs::reread says (-1); the fixed forms keep the branch out of
+// the pair trainer.
+template <int DIM, class P, int RR = -1>
 struct LaneRows {
   static constexpr int J = DIM / 32;
   static constexpr int H = J / 2;
   const float *f[2];     // FP32 rows of syn0 / syn1 with this lane's offset
   const uint16_t *b[2];  // BF16 rows with this lane's offset, shifted so row r is at b + r * DIM
   uint32_t n_hot;
-  bool reread;           // BF16 rows read again right before their store (SgArgs::reread)
+  bool reread;           // RR < 0: SgArgs::reread
 
   __device__ __forceinline__ void init(const SgArgs &a) {
     const int lo = lane_id() * J;
     f[0] = a.syn0 + lo;
     f[1] = a.syn1 + lo;
     n_hot = 0;
-    reread = a.reread != 0;
+    reread = RR < 0 ? a.reread != 0 : RR > 0;
     b[0] = b[1] = nullptr;
     if constexpr (P::kBF16) {
       n_hot = (uint32_t)a.n_hot;
@@ -270,7 +272,7 @@ struct LaneRows {
       return false;
     } else {
       const bool hot = row < n_hot;
-      if (!hot && reread) {
+      if (!hot && (RR < 0 ? reread : RR > 0)) {
         uint32_t hv[H];
         load_b16(b[W] + (size_t)row * DIM, hv);
 #pragma unroll
@@ -408,10 +410,11 @@ __device__ __forceinline__ int rec_at(const int4 (&v)[S / 4], int i) {
 // sees the earlier update as in the reference.
 // MINB: resident 256-thread blocks per SM the register budget is built for
 // (the launch-shape autotuner picks among 2, 3, 4 and 5 for DIM <= 128).
+// RR (BF16 rows): every cold row is read again right before its store.
 // CNT (diagnostic, BF16 rows): every cold-row store bumps the row's version;
 // a store whose row changed version since this warp read it overwrote another
 // warp's update, which is counted as lost.
-template <int DIM, int NK, class P, int MINB = (DIM >= 256 ? 2 : 4), bool CNT = false>
+template <int DIM, int NK, class P, int MINB = (DIM >= 256 ? 2 : 4), bool RR = false, bool CNT = false>
 __global__ void __launch_bounds__(256, MINB)
     k_sgns_train_pairs(SgArgs a, const int32_t *__restrict__ rec, const uint64_t *__restrict__ off, uint64_t base,
                        uint64_t s0) {
@@ -423,7 +426,7 @@ __global__ void __launch_bounds__(256, MINB)
   __shared__ float s_exp[1000];
   load_exp(a, s_exp);
   const int lane = lane_id();
-  LaneRows<DIM, P> rows;
+  LaneRows<DIM, P, RR ? 1 : 0> rows;
   rows.init(a);
   unsigned long long n_cold = 0, n_lost = 0;  // CNT only
   unsigned long long sc;
@@ -482,7 +485,7 @@ __global__ void __launch_bounds__(256, MINB)
               neu[k] = __ffma2_rn(g2, y[q][k], neu[k]);
               upd[k] = __fmul2_rn(g2, x[k]);
             }
-            if constexpr (CNT) if (rows.reread) seen[q] = __ldcg(&a.ver1[tg[q]]);  // the window starts at the re-read
+            if constexpr (CNT && RR) seen[q] = __ldcg(&a.ver1[tg[q]]);  // the window starts at the re-read
             rows.template update<1>((uint32_t)tg[q], upd, y[q], key, (uint32_t)q);
             if constexpr (CNT) count_store(a.ver1, (uint32_t)tg[q], seen[q], rows.n_hot, n_cold, n_lost);
           }
@@ -515,7 +518,7 @@ __global__ void __launch_bounds__(256, MINB)
               for (int k = 0; k < H; k++) y[r][k] = stored ? y[q][k] : __fadd2_rn(y[q][k], upd[k]);
         }
       }
-      if constexpr (CNT) if (rows.reread) seen[NT] = __ldcg(&a.ver0[l1]);
+      if constexpr (CNT && RR) seen[NT] = __ldcg(&a.ver0[l1]);
       rows.template update<0>(l1, neu, x, key, kSlotCtx);
       if constexpr (CNT) count_store(a.ver0, l1, seen[NT], rows.n_hot, n_cold, n_lost);
     }

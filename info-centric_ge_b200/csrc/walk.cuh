@@ -377,9 +377,11 @@ __global__ void __launch_bounds__(kWalkThreads, 3) k_walk(WalkArgs a) {
 // a dependent uniform-neighbour gather (the candidate's adjacency entry, then
 // the neighbour's row_ptr pair) with probability gather_frac (the round's
 // forward steps per token), else a repeat of the current vertex (the return
-// token of a trace, which loads nothing).  Same block size, residency and
-// warp claims as k_walk; no FP64, no trace test, no revisit counts and no
-// visit counters.  Tokens go to a scratch buffer at the walk's offsets.
+// token of a trace, which loads nothing).  Same block size and warp claims
+// as k_walk, at its own full residency (no shared memory and few registers
+// give 8 blocks per SM, where k_walk holds 3); no FP64, no trace test, no
+// revisit counts and no visit counters.  Tokens go to a scratch buffer at
+// the walk's offsets.
 __global__ void __launch_bounds__(kWalkThreads, 3)
     k_walk_skeleton(const uint64_t *__restrict__ row_ptr, const uint2 *__restrict__ adj, uint32_t v_num,
                     uint32_t n_active, const uint32_t *__restrict__ active, const uint64_t *__restrict__ sent_ptr,
