@@ -96,7 +96,7 @@ METRIC = "walk+SGNS corpus tokens/s (walk steps/s and SGNS words/s reported alon
 WALK_BYTES_PER_STEP = 68      # 2 random 32-B sectors + 4-B token write
 # DRAM bytes per pair of k_sgns_train_pairs<128, 5> (dram__bytes_read.sum + dram__bytes_write.sum of one ncu
 # capture of the profiling case's timed round divided by its 66.0 M pairs), scaled to a launch
-DRAM_BYTES_PER_PAIR = {"fp32": 1059.2, "bf16": 242.3}  # bf16: 5 blocks per SM; fp32: 4
+DRAM_BYTES_PER_PAIR = {"fp32": 1055.6, "bf16": 244.1}  # bf16: 5 blocks per SM; fp32: 4
 SGNS_BYTES_PER_PAIR = {"fp32": 7168,   # 14 rows x 128 x 4 B (read + write syn0 row and 6 syn1 rows)
                        "bf16": 3584}   # the same rows at 2 B per value (FP32 master rows: top 1%)
 
@@ -266,6 +266,53 @@ def cpu_baseline(g, cfg):
     return {"value": value, "unit": "tokens/s", "cores": 1, "kind": "port",
             "sample": f"oracle walk of {nw} walkers ({len(tok)} tokens, {t_walk:.1f}s) + skip-gram over "
                       f"{ns} sentences ({int(o2[-1])} tokens, {t_train:.1f}s), 1 thread",
+            "walk_steps_per_s": walk_rate, "sgns_words_per_s": train_rate}
+
+
+def cpu_baseline_resident(f, V, n_walkers=60000, n_sent=1500):
+    """The oracle (CPU restatement, one thread) on a bounded sample of a graph
+    that only the device holds (C5, generated in HBM): the CSR copied out of
+    the context, the walk of the first n_walkers walkers and the skip-gram pass
+    over the first n_sent of their sentences.  syn0 and syn1 span the whole
+    vocabulary but only the rows the sample touches are written (syn1 starts at
+    zero as in InitNet, syn0 rows of the sample's words get the fixed init), so
+    untouched pages are never allocated.  Reported as corpus tokens/s through
+    walk + train."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_binding as ob
+    rp, nb, dt = f.csr()
+
+    class HostCsr:  # the oracle's CSR view of the copied arrays
+        def __init__(self):
+            self.c = ob.Csr(V, len(nb), ob.ptr(rp, ob.u64p), ob.ptr(nb, ob.u32p), ob.ptr(dt, ob.f32p))
+            self.deg = np.diff(rp).astype(np.uint32)
+
+    c = HostCsr()
+    t0 = time.perf_counter()
+    tok, off, _, st = ob.walk_round(c, n_walkers, TRAIN["min_length"], seed=1, round_=0)
+    t_walk = time.perf_counter() - t0
+    vv, vcn, id2, vs, tw = ob.vocab(c.deg, 0)
+    thr, used = ob.subsample_thresholds(vcn, TRAIN["sample"], tw)
+    table = ob.unigram_table(vcn)
+    et = ob.exp_table()
+    dim = TRAIN["size"]
+    syn0 = np.zeros(vs * dim, np.float32)
+    syn1 = np.zeros(vs * dim, np.float32)
+    t2, o2 = tok[: int(off[n_sent])], off[: n_sent + 1]
+    rows = np.unique(id2[t2]).astype(np.int64)
+    s0 = syn0.reshape(vs, dim)
+    s0[rows] = ((rows[:, None] * dim + np.arange(dim)[None, :]) % 97 - 48).astype(np.float32) / (97 * dim)
+    pl = ob.plan_batches(t2, o2, id2, thr, used, table, vs, TRAIN["negative"])
+    t1 = time.perf_counter()
+    ob.skipgram_batch(syn0, syn1, et, table, vs, pl["sen"], pl["sent_start"], 0, len(pl["sent_start"]) - 1,
+                      TRAIN["window"], dim, TRAIN["negative"], 0.025)
+    t_train = time.perf_counter() - t1
+    walk_rate = len(tok) / t_walk
+    train_rate = int(o2[-1]) / t_train
+    return {"value": 1.0 / (1.0 / walk_rate + 1.0 / train_rate), "unit": "tokens/s", "cores": 1, "kind": "port",
+            "sample": f"oracle walk of {n_walkers} walkers on the C5 CSR copied out of HBM ({len(tok)} tokens, "
+                      f"{t_walk:.1f}s) + skip-gram over {n_sent} sentences ({int(o2[-1])} tokens, {t_train:.1f}s), "
+                      f"1 thread",
             "walk_steps_per_s": walk_rate, "sgns_words_per_s": train_rate}
 
 
@@ -609,8 +656,14 @@ def bench_streamed(args):
     job = f.run()
     f.embeddings_into(emb.ctypes.data, emb.size)
     e2e_s = time.perf_counter() - t0
-    f.close()
     del emb
+    cpu = None
+    if not args.no_cpu_baseline:
+        try:
+            cpu = cpu_baseline_resident(f, V)
+        except Exception as ex:  # reported, not fatal
+            cpu = {"error": str(ex)}
+    f.close()
     out = {
         "metric": METRIC, "value": cnt["tokens"] / (ms * 1e-3), "unit": "tokens/s", "n_gpus": 1,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
@@ -622,15 +675,17 @@ def bench_streamed(args):
                    "undirected_edges": info["n_edges"], "max_degree": info["max_degree"], "dim": 128, "window": 10,
                    "negative": 5, "sample": 1e-3, "min_L": 20, "min_R": 2, "skip_gram": True, "precision": prec,
                    "step": f"one piece of {piece} walkers of a round: walk, plan, pair stream, train",
-                   "unigram_table_slots": "2^30 (8 per word; the reference's 1e8 below 12.5M words)",
+                   "unigram_table_slots": f"2^{max(8 * vs - 1, 1).bit_length()} (the power of two >= 8 per word; "
+                                          "the reference's 1e8 below 12.5M words)",
                    "l2": "inputs larger than L2", "parallelism": "replicas x1", "graph_gen_s": gen_s},
         "walk_steps_per_s": cnt["tokens"] / (cnt["walk_ms"] * 1e-3),
         "sgns_words_per_s": cnt["words"] / ((cnt["train_ms"] + cnt["plan_ms"]) * 1e-3),
         "phase_ms_per_step": {k: cnt[k] / args.steps for k in ("walk_ms", "plan_ms", "train_ms")},
         "tokens_per_step": cnt["tokens"] / args.steps, "pairs_per_step": cnt["pairs"] / args.steps,
         "roofline": {"kernel": f"k_sgns_train_pairs<128, 5, Rows{prec.upper()}>", "bound": "hbm",
-                     "traffic": DRAM_BYTES_PER_PAIR[prec] * cnt["pairs"] / args.steps,
-                     "traffic_unit": "bytes per step (ncu per-pair DRAM traffic of the profiling case x pairs)",
+                     "traffic": DRAM_BYTES_PER_PAIR[prec] * min(cnt["pairs"] / args.steps, 2 ** 27),
+                     "traffic_unit": "bytes per launch (ncu per-pair DRAM traffic of the profiling case x pairs "
+                                     "per launch: one 2^27-pair chunk)",
                      "achieved": sg_achieved, "peak": peak, "unit": "GB/s", "frac": sg_achieved / peak,
                      "algorithmic_bytes_per_pair": refs_per_pair * per_ref, "row_refs_per_pair": refs_per_pair,
                      "master_row_share": hot_share, "peak_source": peak_kind,
@@ -643,6 +698,8 @@ def bench_streamed(args):
         "gpu_launches": int(launches),
         "clocks": clk.summary(),
     }
+    if cpu is not None:
+        out["cpu_baseline"] = cpu
     if not args.no_forms:
         forms = {}
         for fm in ("plain-fp32", "learned-bf16"):

@@ -674,11 +674,16 @@ extern "C" felog_status felog_get_csr(felog_ctx *c, uint64_t *row_ptr, uint32_t 
   if (row_ptr)
     CK(cudaMemcpy(row_ptr, c->row_ptr.p, sizeof(uint64_t) * (c->V + 1ULL), cudaMemcpyDeviceToHost), "get_csr");
   if ((nbr || data) && c->M) {
-    std::vector<uint2> a(c->M);
-    CK(cudaMemcpy(a.data(), c->adj.p, sizeof(uint2) * c->M, cudaMemcpyDeviceToHost), "get_csr");
-    for (uint64_t i = 0; i < c->M; i++) {
-      if (nbr) nbr[i] = a[i].x;
-      if (data) memcpy(&data[i], &a[i].y, 4);
+    // in pieces of 2^26 entries (512 MiB), so a 3.2 G-entry CSR needs no host copy of its own
+    const uint64_t piece = std::min<uint64_t>(c->M, 1ull << 26);
+    std::vector<uint2> a(piece);
+    for (uint64_t b = 0; b < c->M; b += piece) {
+      const uint64_t n = std::min(piece, c->M - b);
+      CK(cudaMemcpy(a.data(), c->adj.p + b, sizeof(uint2) * n, cudaMemcpyDeviceToHost), "get_csr");
+      for (uint64_t i = 0; i < n; i++) {
+        if (nbr) nbr[b + i] = a[i].x;
+        if (data) memcpy(&data[b + i], &a[i].y, 4);
+      }
     }
   }
   return FELOG_OK;
