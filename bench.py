@@ -90,6 +90,9 @@ FORMS = {
     "learned-fp32-tile": dict(precision=0, budget_mode=1, reuse_neg=2),
     # BF16 tables + learned budget + center tiles scored on the tensor cores
     "learned-bf16-tc": dict(precision=1, budget_mode=1, reuse_neg=3),
+    # BF16 tables + learned budget, -reuse-neg 4 window tiles (the skip-gram windows; each center's
+    # contexts share the K negatives drawn for its first context)
+    "learned-bf16-window": dict(precision=1, budget_mode=1, reuse_neg=4),
 }
 BUDGET_MODEL = os.path.join(ROOT, "info-centric_ge_b200", "felog_b200", "budget_mlp_c4.npy")
 METRIC = "walk+SGNS corpus tokens/s (walk steps/s and SGNS words/s reported alongside)"
@@ -354,6 +357,9 @@ def reference_quality(g, pairs):
             "wall_s": time.perf_counter() - t0}
 
 
+FORM_SET = ("plain-fp32", "learned-bf16", "learned-bf16-window", "learned-bf16-tile", "learned-fp32-tile")
+
+
 def compare_forms(fb, g, device, model):
     """Plain FP32 and learned-budget BF16, each run end to end (felog_run: walk,
     train and budget check until the stop-all rule) on the same graph and walk
@@ -363,7 +369,7 @@ def compare_forms(fb, g, device, model):
     import ref_tables as rt
     pairs = rt.fit_pairs(g)
     out = {}
-    for form in ("plain-fp32", "learned-bf16", "learned-bf16-tile", "learned-fp32-tile"):
+    for form in FORM_SET:
         f = new_context(fb, g, form, device, 77, model)
         f.run()         # untimed first run: device allocations and first-use module loading
         f.init_model()  # the timed run starts over from InitNet with the same walk seed
@@ -377,7 +383,7 @@ def compare_forms(fb, g, device, model):
         out[form].update(quality(f, g, pairs))
         f.close()
     p = out["plain-fp32"]
-    for form in ("learned-bf16", "learned-bf16-tile", "learned-fp32-tile"):
+    for form in FORM_SET[1:]:
         out[form]["end_to_end_speedup_vs_plain_fp32"] = p["job_ms"] / out[form]["job_ms"]
         for k in ("auc", "auc_centered", "fit_auc", "fit_auc_sgns"):
             out[form][k + "_delta_vs_plain_fp32"] = out[form][k] - p[k]
@@ -492,10 +498,11 @@ def bench_mine(args):
     peak, peak_kind = measured_peaks()
     # dominant kernel: the skip-gram pass
     row_bytes = SGNS_BYTES_PER_PAIR[prec] // 14
-    if FORMS[form]["reuse_neg"] == 2:
+    if FORMS[form]["reuse_neg"] in (2, 4):
         # center tiles: per center its contexts and the K + 1 targets, each read and written once
         sg_bytes = 2 * row_bytes * (cnt["pairs"] + (TRAIN["negative"] + 1) * cnt["words"])  # words: centers before subsampling (an upper bound)
-        sg_kernel = f"k_sgns_reuse_tile<128, 5, Rows{prec.upper()}>"
+        sg_kernel = (f"k_sgns_reuse_tile<128, 5, Rows{prec.upper()}" +
+                     (", true>" if FORMS[form]["reuse_neg"] == 4 else ">"))
     elif FORMS[form]["reuse_neg"] == 3:
         sg_bytes = 2 * row_bytes * (cnt["pairs"] + (TRAIN["negative"] + 1) * cnt["words"])  # words: centers before subsampling (an upper bound)
         sg_kernel = "k_sgns_reuse_tile_tc<128, 5>"

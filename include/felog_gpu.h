@@ -81,7 +81,9 @@ typedef struct felog_opts {
   int32_t hs;               /* -hs (must be 0) */
   int32_t cbow;             /* -cbow */
   int32_t reuse_neg;        /* -reuse-neg: 1 the reference's pair order; B200 options: 2 one tile per center,
-                               3 center tiles scored on the tensor cores (BF16 form) */
+                               3 center tiles scored on the tensor cores (BF16 form), 4 window tiles (the
+                               skip-gram windows and draws, each center sharing its first context's K
+                               negatives across its contexts) */
   int32_t iter;             /* -iter (parsed, unused like the reference) */
   int32_t min_count;        /* -min-count */
   int32_t classes;          /* -classes (K-means output) */

@@ -33,7 +33,7 @@ void usage() {
           "usage: felog -g <graph.bin> -v <V> -w <walkers> --min_L <L> --min_R <R> -o <prefix>\n"
           "             [--make-undirected] [-p <partition>] [--batch_size <n>] [-r <rate>]\n"
           "             [-size n] [-window n] [-negative n] [-sample x] [-alpha x] [-cbow 0|1]\n"
-          "             [-reuse-neg 0|1|2|3] [-hs 0] [-iter n] [-min-count n] [-classes k] [-binary 0|1]\n"
+          "             [-reuse-neg 0|1|2|3|4] [-hs 0] [-iter n] [-min-count n] [-classes k] [-binary 0|1]\n"
           "             [-debug n] [-save-vocab f] [-emb_output f]\n"
           "             [--use-cli-alpha] [--precision fp32|bf16] [--budget plain|learned] [--budget-model f]\n"
           "             [--seed n] [--deterministic] [--weighted] [--max-rounds n] [--device n]\n");

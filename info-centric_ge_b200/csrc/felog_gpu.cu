@@ -1638,6 +1638,28 @@ void launch_pairs_kp(felog_ctx *c, const SgArgs &g, int blocks, int threads, uin
   }
 }
 
+// The negative LCG advanced by K j steps, j = 0 .. 2 window (a center with j
+// contexts draws K j times): x -> pr_jump[j] x + pr_jump[2 window + 1 + j]
+felog_status ensure_jump(felog_ctx *c, const SgArgs &g) {
+  const int K = c->o.negative;
+  const int nj = 2 * c->o.window + 1;
+  if (c->pr_jump_window != c->o.window || c->pr_jump_k != K) {
+    std::vector<unsigned long long> jt(2 * (size_t)nj);
+    unsigned long long A = 1, C = 0;
+    for (int j = 0; j < nj; j++) {
+      jt[j] = A;
+      jt[nj + j] = C;
+      A = A * g.lcg_a[K - 1];
+      C = C * g.lcg_a[K - 1] + g.lcg_c[K - 1];
+    }
+    CK(c->pr_jump.ensure(2 * (size_t)nj), "train: jump table");
+    CK(cudaMemcpy(c->pr_jump.p, jt.data(), 8 * jt.size(), cudaMemcpyHostToDevice), "train: jump table");
+    c->pr_jump_window = c->o.window;
+    c->pr_jump_k = K;
+  }
+  return FELOG_OK;
+}
+
 // Skip-gram with K = 5 or 7 over the pair stream: count the pairs of every
 // sentence, scan, then per chunk of at most kPairChunk pairs emit the records
 // and train them.
@@ -1660,24 +1682,10 @@ felog_status train_pairs(felog_ctx *c, SgArgs g, int blocks, int threads) {
   pa.window = c->o.window;
   pa.negative = K;
   pa.stride = stride;
-  // the negative LCG advanced by K j steps, j = 0 .. 2 window
-  const int nj = 2 * c->o.window + 1;
-  if (c->pr_jump_window != c->o.window || c->pr_jump_k != K) {
-    std::vector<unsigned long long> jt(2 * (size_t)nj);
-    unsigned long long A = 1, C = 0;
-    for (int j = 0; j < nj; j++) {
-      jt[j] = A;
-      jt[nj + j] = C;
-      A = A * g.lcg_a[K - 1];
-      C = C * g.lcg_a[K - 1] + g.lcg_c[K - 1];
-    }
-    CK(c->pr_jump.ensure(2 * (size_t)nj), "train: jump table");
-    CK(cudaMemcpy(c->pr_jump.p, jt.data(), 8 * jt.size(), cudaMemcpyHostToDevice), "train: jump table");
-    c->pr_jump_window = c->o.window;
-    c->pr_jump_k = K;
-  }
+  felog_status js = ensure_jump(c, g);
+  if (js != FELOG_OK) return js;
   pa.jump_a = c->pr_jump.p;
-  pa.jump_c = c->pr_jump.p + nj;
+  pa.jump_c = c->pr_jump.p + 2 * c->o.window + 1;
   CK(c->pr_cstate.ensure(c->plan_sen + 1), "train: center states");
   CK(c->pr_cfirst.ensure(c->plan_sen + 1), "train: center offsets");
   pa.cstate = c->pr_cstate.p;
@@ -1811,8 +1819,9 @@ extern "C" felog_status felog_train_round(felog_ctx *c, uint32_t round, float al
   // -reuse-neg applies to skip-gram only; with -cbow 1 the CBOW kernel runs (word2vec.cu:1255-1258)
   if (c->o.reuse_neg && !c->o.cbow && (c->o.size < 64 || (c->o.negative != 5 && c->o.negative != 7)))
     return fail(c, FELOG_INVALID_ARG, "-reuse-neg runs skip-gram with -negative 5 or 7 and -size >= 64");
-  if (c->o.reuse_neg < 0 || c->o.reuse_neg > 3)
-    return fail(c, FELOG_INVALID_ARG, "-reuse-neg %d: 0, 1 (pair order), 2 (center tiles) or 3 (tensor-core tiles)",
+  if (c->o.reuse_neg < 0 || c->o.reuse_neg > 4)
+    return fail(c, FELOG_INVALID_ARG,
+                "-reuse-neg %d: 0, 1 (pair order), 2 (center tiles), 3 (tensor-core tiles) or 4 (window tiles)",
                 c->o.reuse_neg);
   if (c->o.reuse_neg == 3 && !c->o.cbow &&
       (c->o.precision != FELOG_BF16 || (c->o.size != 64 && c->o.size != 128) || 2 * c->o.window > kTileRows))
@@ -1881,13 +1890,28 @@ extern "C" felog_status felog_train_round(felog_ctx *c, uint32_t round, float al
     else k_sgns_reuse_tile_tc<128, 7><<<tb, tt, 0, c->stream>>>(g);
     c->launches++;
     CK(cudaGetLastError(), "train_round: launch");
-  } else if (!c->o.cbow && c->o.reuse_neg == 2) {
-    // center tiles over the plan negatives (k_sgns_reuse_tile)
+  } else if (!c->o.cbow && (c->o.reuse_neg == 2 || c->o.reuse_neg == 4)) {
+    // center tiles over the plan negatives (2) or over the skip-gram windows and
+    // each center's first draws (4, window tiles) (k_sgns_reuse_tile)
     const bool bf = c->o.precision == FELOG_BF16;
-#define FELOG_RT(D, K)                                                                      \
-  do {                                                                                      \
-    if (bf) k_sgns_reuse_tile<D, K, RowsBF16><<<blocks, threads, 0, c->stream>>>(g);       \
-    else k_sgns_reuse_tile<D, K, RowsF32><<<blocks, threads, 0, c->stream>>>(g);           \
+    const bool win = c->o.reuse_neg == 4;
+    if (win) {
+      s = ensure_jump(c, g);
+      if (s != FELOG_OK) return s;
+      g.jump_a = c->pr_jump.p;
+      g.jump_c = c->pr_jump.p + 2 * c->o.window + 1;
+      g.coarse = c->table_coarse.p;
+      g.fm_table = make_fastmod((uint32_t)c->table_size);
+    }
+#define FELOG_RT(D, K)                                                                             \
+  do {                                                                                             \
+    if (win) {                                                                                     \
+      if (bf) k_sgns_reuse_tile<D, K, RowsBF16, true><<<blocks, threads, 0, c->stream>>>(g);      \
+      else k_sgns_reuse_tile<D, K, RowsF32, true><<<blocks, threads, 0, c->stream>>>(g);          \
+    } else {                                                                                       \
+      if (bf) k_sgns_reuse_tile<D, K, RowsBF16><<<blocks, threads, 0, c->stream>>>(g);            \
+      else k_sgns_reuse_tile<D, K, RowsF32><<<blocks, threads, 0, c->stream>>>(g);                \
+    }                                                                                              \
   } while (0)
     const int K = c->o.negative, D = c->o.size;
     if (K == 5 && D == 64) FELOG_RT(64, 5);

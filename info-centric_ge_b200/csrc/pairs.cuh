@@ -538,7 +538,14 @@ __global__ void __launch_bounds__(256, MINB)
 // center (a negative that occurs twice gets the sum of both).  Per center this
 // reads and writes n + K + 1 rows instead of 2 (K + 1) n for the pair-by-pair
 // order, n being the number of contexts.
-template <int DIM, int NK, class P>
+//
+// WIN (-reuse-neg 4, window tiles): the same tile over skip_gram_kernel's own
+// windows (word2vec.cu:442-536): the window shrink b comes from the
+// sentence's LCG (:458-459) and the center's shared negatives are the K draws
+// the reference makes for its first context (:496-507); the LCG then jumps
+// past the K draws of every context of the center, so every center's window
+// is the reference's.  Lane q < K makes draw q; one table lookup per lane.
+template <int DIM, int NK, class P, bool WIN = false>
 __global__ void __launch_bounds__(256, 4) k_sgns_reuse_tile(SgArgs a) {
   static_assert(DIM >= 64, "two or more values per lane");
   constexpr int H = DIM / 64;
@@ -554,14 +561,36 @@ __global__ void __launch_bounds__(256, 4) k_sgns_reuse_tile(SgArgs a) {
   while (claim_sentence(a, s)) {
     const long long sb = (long long)a.sent_start[s], se = (long long)a.sent_start[s + 1];
     int neg[NK];
+    unsigned long long nr = 0;  // WIN: the sentence's LCG, seeded by its index in the batch (word2vec.cu:446)
+    if constexpr (WIN) {
+      nr = a.blk[s];
+    } else {
 #pragma unroll
-    for (int q = 0; q < NK; q++) neg[q] = __ldg(&a.negs[s * (uint64_t)NK + q]);
+      for (int q = 0; q < NK; q++) neg[q] = __ldg(&a.negs[s * (uint64_t)NK + q]);
+    }
     for (long long pos = sb; pos < se; pos++) {
       const int word = __ldg(&a.sen[pos]);
-      long long c0 = pos - a.window, c1 = pos + a.window;
+      int b = 0;
+      if constexpr (WIN) {
+        nr = nr * 2514903917ULL + 11ULL;
+        b = (int)fastmod(nr, a.fm_window);
+      }
+      long long c0 = pos - a.window + b, c1 = pos + a.window - b;
       if (c0 < sb) c0 = sb;
       if (c1 > se - 1) c1 = se - 1;
-      if (c1 - c0 < 1) continue;  // no context
+      if (c1 - c0 < 1) continue;  // no context, no draws
+      if constexpr (WIN) {
+        int v = 0;
+        if (lane < NK) {
+          const unsigned long long r = a.lcg_a[lane] * nr + a.lcg_c[lane];
+          v = unigram_lookup(a.table, a.coarse, fastmod(r >> 16, a.fm_table));
+          if (v == 0) v = (int)fastmod(r, a.fm_vocab1) + 1;
+        }
+#pragma unroll
+        for (int q = 0; q < NK; q++) neg[q] = __shfl_sync(0xffffffffu, v, q);
+        const int n = (int)(c1 - c0);
+        nr = __ldg(&a.jump_a[n]) * nr + __ldg(&a.jump_c[n]);
+      }
       int tg[NT];
       tg[0] = word;
 #pragma unroll

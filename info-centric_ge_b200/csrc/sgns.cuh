@@ -87,6 +87,11 @@ struct SgArgs {
   // BF16 rows are read again right before their store, so a concurrent
   // update lands in the stored value unless it falls in that last round trip
   int reread;
+  // window tiles (-reuse-neg 4): the unigram table's coarse buckets, % slots,
+  // and the negative LCG advanced by K j steps (j = 0 .. 2 window)
+  const uint32_t *coarse;
+  FastMod fm_table;
+  const unsigned long long *jump_a, *jump_c;
 };
 
 // ------------------------------------------------------------ row access

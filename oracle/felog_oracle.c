@@ -718,23 +718,43 @@ void orc_negreuse_bf16(float *syn0, uint16_t *syn0_bf, float *syn1, uint16_t *sy
  * vocab_size: all FP32); rounding streams as orc_skipgram_bf16 with the
  * center's index in the sentence as the pair index, slot j for targets and
  * 256 + window position for contexts. */
-void orc_negreuse_tile(float *syn0, uint16_t *syn0_bf, float *syn1, uint16_t *syn1_bf, long long n_hot,
-                       uint32_t sr_seed, const float *exp_table, const int32_t *sen, const uint64_t *sent_start,
-                       uint64_t first_sentence, uint64_t n_sentences, const int32_t *negs, int window, int dim,
-                       int negative, float alpha) {
+static void tile_impl(float *syn0, uint16_t *syn0_bf, float *syn1, uint16_t *syn1_bf, long long n_hot,
+                      uint32_t sr_seed, const float *exp_table, const int32_t *table, int64_t table_size,
+                      long long vocab_size, const int32_t *sen, const uint64_t *sent_start, uint64_t first_sentence,
+                      uint64_t n_sentences, const int32_t *negs, int window, int dim, int negative, float alpha) {
   mixed_rows m0 = {syn0, syn0_bf, n_hot, dim}, m1 = {syn1, syn1_bf, n_hot, dim};
   float x[512], neu1e[512];
   float y[16][512], dy[16][512];
-  int tg[16];
+  int tg[16], wneg[16];
   for (uint64_t blk = 0; blk < n_sentences; blk++) {
     uint64_t s = first_sentence + blk;
     long long ss = (long long)sent_start[s], se = (long long)sent_start[s + 1];
-    const int32_t *neg = negs + s * (uint64_t)negative;
+    const int32_t *neg = negs ? negs + s * (uint64_t)negative : wneg;
+    unsigned long next_random = (unsigned long)blk;
     for (long long pos = ss; pos < se; pos++) {
       int word = sen[pos];
-      long long c0 = pos - window < ss ? ss : pos - window;
-      long long c1 = pos + window > se - 1 ? se - 1 : pos + window;
+      int b = 0;
+      if (!negs) {
+        next_random = next_random * (unsigned long)2514903917 + 11;
+        b = (int)(next_random % (unsigned long)window);
+      }
+      long long c0 = pos - window + b < ss ? ss : pos - window + b;
+      long long c1 = pos + window - b > se - 1 ? se - 1 : pos + window - b;
       if (c1 - c0 < 1) continue;
+      if (!negs) {
+        /* skip_gram_kernel draws K negatives per context (word2vec.cu:496-507);
+         * the center keeps the draws of its first context and the stream moves
+         * on past all of its contexts' draws */
+        for (long long c = c0; c <= c1; c++) {
+          if (c == pos) continue;
+          for (int q = 0; q < negative; q++) {
+            next_random = next_random * (unsigned long)25214903917 + 11;
+            int t = table[(next_random >> 16) % (unsigned long)table_size];
+            if (t == 0) t = (int)(next_random % (unsigned long)(vocab_size - 1) + 1);
+            if (c == (c0 == pos ? c0 + 1 : c0)) wneg[q] = t;
+          }
+        }
+      }
       int nt = negative + 1;
       tg[0] = word;
       for (int q = 0; q < negative; q++) tg[q + 1] = neg[q] == word ? -1 : neg[q];
@@ -772,6 +792,30 @@ void orc_negreuse_tile(float *syn0, uint16_t *syn0_bf, float *syn1, uint16_t *sy
         if (tg[q] >= 0) mr_add(&m1, tg[q], y[q], dy[q], sr_seed, s, center, (uint32_t)q);
     }
   }
+}
+
+void orc_negreuse_tile(float *syn0, uint16_t *syn0_bf, float *syn1, uint16_t *syn1_bf, long long n_hot,
+                       uint32_t sr_seed, const float *exp_table, const int32_t *sen, const uint64_t *sent_start,
+                       uint64_t first_sentence, uint64_t n_sentences, const int32_t *negs, int window, int dim,
+                       int negative, float alpha) {
+  tile_impl(syn0, syn0_bf, syn1, syn1_bf, n_hot, sr_seed, exp_table, NULL, 0, 0, sen, sent_start, first_sentence,
+            n_sentences, negs, window, dim, negative, alpha);
+}
+
+/* -reuse-neg 4 (this project's option): window tiles.  The center tile of
+ * orc_negreuse_tile over skip_gram_kernel's own window and draws
+ * (word2vec.cu:442-536): the window shrink b from the sentence's LCG
+ * (:458-459), contexts pos - window + b .. pos + window - b, and as the
+ * center's shared negatives the K draws the reference makes for the center's
+ * first context (:496-507, 0 -> next % (vocab - 1) + 1, skipped when equal to
+ * the word); the LCG then advances past the K draws of every context, so each
+ * center's window is the reference's. */
+void orc_window_tile(float *syn0, uint16_t *syn0_bf, float *syn1, uint16_t *syn1_bf, long long n_hot,
+                     uint32_t sr_seed, const float *exp_table, const int32_t *table, int64_t table_size,
+                     long long vocab_size, const int32_t *sen, const uint64_t *sent_start, uint64_t first_sentence,
+                     uint64_t n_sentences, int window, int dim, int negative, float alpha) {
+  tile_impl(syn0, syn0_bf, syn1, syn1_bf, n_hot, sr_seed, exp_table, table, table_size, vocab_size, sen, sent_start,
+            first_sentence, n_sentences, NULL, window, dim, negative, alpha);
 }
 
 /* -reuse-neg 3 (this project's option, BF16 form): the center tile scored on

@@ -152,6 +152,10 @@ void orc_negreuse_tile(float *syn0, uint16_t *syn0_bf, float *syn1, uint16_t *sy
                        uint32_t sr_seed, const float *exp_table, const int32_t *sen, const uint64_t *sent_start,
                        uint64_t first_sentence, uint64_t n_sentences, const int32_t *negs, int window, int dim,
                        int negative, float alpha);
+void orc_window_tile(float *syn0, uint16_t *syn0_bf, float *syn1, uint16_t *syn1_bf, long long n_hot,
+                     uint32_t sr_seed, const float *exp_table, const int32_t *table, int64_t table_size,
+                     long long vocab_size, const int32_t *sen, const uint64_t *sent_start, uint64_t first_sentence,
+                     uint64_t n_sentences, int window, int dim, int negative, float alpha);
 void orc_negreuse_tile_tc(float *syn0, uint16_t *syn0_bf, float *syn1, uint16_t *syn1_bf, long long n_hot,
                           uint32_t sr_seed, const float *exp_table, const int32_t *sen, const uint64_t *sent_start,
                           uint64_t first_sentence, uint64_t n_sentences, const int32_t *negs, int window, int dim,

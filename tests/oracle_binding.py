@@ -90,6 +90,7 @@ def lib():
                                         ctypes.c_uint64, ctypes.c_uint64, i32p, ctypes.c_int, ctypes.c_int,
                                         ctypes.c_int, ctypes.c_float]
         L.orc_negreuse_tile_tc.argtypes = L.orc_negreuse_tile.argtypes
+        L.orc_window_tile.argtypes = L.orc_skipgram_bf16.argtypes
         L.orc_negreuse_bf16.argtypes = [f32p, u16p, f32p, u16p, ctypes.c_longlong, ctypes.c_uint32, f32p, i32p, u64p,
                                         ctypes.c_uint64, ctypes.c_uint64, i32p, ctypes.c_int, ctypes.c_int,
                                         ctypes.c_int, ctypes.c_float]
@@ -316,6 +317,17 @@ def negreuse_tile(m0, m1, sr_seed, exp_tab, sen, sent_start, first, n, negs, win
                             sr_seed, ptr(exp_tab, f32p), ptr(np.ascontiguousarray(sen, np.int32), i32p),
                             ptr(np.ascontiguousarray(sent_start, np.uint64), u64p), first, n,
                             ptr(np.ascontiguousarray(negs, np.int32), i32p), window, dim, negative, alpha)
+
+
+def window_tile(m0, m1, sr_seed, exp_tab, table, vocab_size, sen, sent_start, first, n, window, dim, negative,
+                alpha):
+    """-reuse-neg 4 window tiles (skip-gram windows, the first context's draws as the
+    center's shared negatives) on MixedRows."""
+    lib().orc_window_tile(ptr(m0.f32, f32p), ptr(m0.bf, u16p), ptr(m1.f32, f32p), ptr(m1.bf, u16p), m0.n_hot,
+                          sr_seed, ptr(exp_tab, f32p), ptr(table, i32p), len(table), vocab_size,
+                          ptr(np.ascontiguousarray(sen, np.int32), i32p),
+                          ptr(np.ascontiguousarray(sent_start, np.uint64), u64p), first, n, window, dim, negative,
+                          alpha)
 
 
 def negreuse_tile_tc(m0, m1, sr_seed, exp_tab, sen, sent_start, first, n, negs, window, dim, negative, alpha):

@@ -135,6 +135,48 @@ def test_reuse_tile_deterministic_matches_oracle(precision, dim, negative):
     assert exact == (1.0, 1.0), f"fraction bit-exact syn0/syn1: {exact}"
 
 
+@pytest.mark.parametrize("precision,dim,negative,window", [(0, 128, 5, 10), (1, 128, 5, 10), (1, 64, 7, 5),
+                                                            (0, 256, 5, 3)])
+def test_window_tile_deterministic_matches_oracle(precision, dim, negative, window):
+    """-reuse-neg 4 (window tiles: skip-gram windows, each center's first draws
+    shared by its contexts) in the one-warp mode against the oracle."""
+    e, V = graph4096()
+    f = fb.Felog(v_num=V, size=dim, window=window, negative=negative, sample=1e-3, cbow=0, reuse_neg=4,
+                 min_count=0, precision=precision, deterministic=1, seed=SEED)
+    f.load_graph(e, V)
+    f.init_model()
+    _, _, vs, _ = f.vocab()
+    nh = n_hot(vs) if precision else vs
+    o0, o1 = ob.init_net(vs, dim)
+    m0, m1 = ob.MixedRows(o0, vs, dim, nh), ob.MixedRows(o1, vs, dim, nh)
+    tok, off = walk_corpus(V, e, 300, seed=8)
+    f.set_corpus(tok, off)
+    st = f.train_round(0, alpha=0.025)
+    c = ob.OracleCsr(e, V)
+    vv, vcn, id2, _, tw = ob.vocab(c.deg, 0)
+    thr, used = ob.subsample_thresholds(vcn, 1e-3, tw)
+    table = ob.unigram_table(vcn)
+    pl = ob.plan_batches(tok, off, id2, thr, used, table, vs, negative)
+    bf = pl["batch_first"]
+    for b in range(len(bf) - 1):
+        ob.window_tile(m0, m1, ob.round_sr_seed(SEED, 0), ob.exp_table(), table, vs, pl["sen"], pl["sent_start"],
+                       int(bf[b]), int(bf[b + 1] - bf[b]), window, dim, negative, 0.025)
+    g0, g1 = f.embeddings()
+    assert not np.array_equal(m0.full(), ob.MixedRows(o0, vs, dim, nh).full())  # training moved the rows
+    exact = np.mean(g0 == m0.full()), np.mean(g1 == m1.full())
+    assert exact == (1.0, 1.0), f"fraction bit-exact syn0/syn1: {exact}"
+    # the windows are the skip-gram windows: as many pairs as the pair stream trains
+    f2 = fb.Felog(v_num=V, size=dim, window=window, negative=negative, sample=1e-3, cbow=0, reuse_neg=0,
+                  min_count=0, precision=precision, deterministic=1, seed=SEED)
+    f2.load_graph(e, V)
+    f2.init_model()
+    f2.set_corpus(tok, off)
+    st2 = f2.train_round(0, alpha=0.025)
+    assert st["pairs"] == st2["pairs"] > 0
+    f.close()
+    f2.close()
+
+
 @pytest.mark.parametrize("dim,negative", [(128, 5), (64, 7)])
 def test_reuse_tile_tensor_core_matches_oracle(dim, negative):
     """-reuse-neg 3 (BF16 form, center tiles scored by mma.sync bf16) in the
