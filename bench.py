@@ -505,7 +505,7 @@ def bench_mine(args):
                      (", true>" if FORMS[form]["reuse_neg"] == 4 else ">"))
     elif FORMS[form]["reuse_neg"] == 3:
         sg_bytes = 2 * row_bytes * (cnt["pairs"] + (TRAIN["negative"] + 1) * cnt["words"])  # words: centers before subsampling (an upper bound)
-        sg_kernel = "k_sgns_reuse_tile_tc<128, 5>"
+        sg_kernel = "k_sgns_tile_umma<128, 5>"
     else:
         # per pair: each referenced row (context + trained targets) read and
         # written once; in the BF16 form the top-1% rows are FP32 master rows,

@@ -28,6 +28,7 @@
 #include "plan.cuh"
 #include "rmat.cuh"
 #include "sgns.cuh"
+#include "umma.cuh"
 #include "walk.cuh"
 
 using namespace felog;
@@ -1859,6 +1860,7 @@ extern "C" felog_status felog_train_round(felog_ctx *c, uint32_t round, float al
   g.syn0_bf = c->syn0_bf.p;
   g.syn1_bf = c->syn1_bf.p;
   g.n_hot = c->n_f32;
+  g.err = c->derr.p;
   // re-read before store: asked for, or automatic below 2^17 vocabulary rows, where
   // thousands of warps share few rows and plain stores would overwrite most concurrent updates
   g.reread = c->o.precision == FELOG_BF16 &&
@@ -1880,14 +1882,23 @@ extern "C" felog_status felog_train_round(felog_ctx *c, uint32_t round, float al
   const int threads = c->o.deterministic ? 32 : 256;
   CK(cudaEventRecord(c->ev0, c->stream), "train_round");
   if (!c->o.cbow && c->o.reuse_neg == 3) {
-    // center tiles scored on the tensor cores (k_sgns_reuse_tile_tc)
-    const int tb = c->o.deterministic ? 1 : c->sm_count * 16;
-    const int tt = c->o.deterministic ? 32 : 32 * kTileWarps;
+    // center tiles scored by tcgen05.mma, four centers (one per warp) per CTA
+    // (k_sgns_tile_umma); one working warp in the deterministic mode
+    const int tb = c->o.deterministic ? 1 : c->sm_count * 4;
+    const int workers = c->o.deterministic ? 1 : kUmmaWarps;
     const int K = c->o.negative, D = c->o.size;
-    if (K == 5 && D == 64) k_sgns_reuse_tile_tc<64, 5><<<tb, tt, 0, c->stream>>>(g);
-    else if (K == 5 && D == 128) k_sgns_reuse_tile_tc<128, 5><<<tb, tt, 0, c->stream>>>(g);
-    else if (K == 7 && D == 64) k_sgns_reuse_tile_tc<64, 7><<<tb, tt, 0, c->stream>>>(g);
-    else k_sgns_reuse_tile_tc<128, 7><<<tb, tt, 0, c->stream>>>(g);
+#define FELOG_UMMA(DD, KK)                                                                                      \
+  do {                                                                                                         \
+    CK(cudaFuncSetAttribute(k_sgns_tile_umma<DD, KK>, cudaFuncAttributeMaxDynamicSharedMemorySize,             \
+                            (int)UmmaSmem<DD>::kDynamic),                                                      \
+       "train_round: tile shared memory");                                                                     \
+    k_sgns_tile_umma<DD, KK><<<tb, 32 * kUmmaWarps, UmmaSmem<DD>::kDynamic, c->stream>>>(g, workers);         \
+  } while (0)
+    if (K == 5 && D == 64) FELOG_UMMA(64, 5);
+    else if (K == 5 && D == 128) FELOG_UMMA(128, 5);
+    else if (K == 7 && D == 64) FELOG_UMMA(64, 7);
+    else FELOG_UMMA(128, 7);
+#undef FELOG_UMMA
     c->launches++;
     CK(cudaGetLastError(), "train_round: launch");
   } else if (!c->o.cbow && (c->o.reuse_neg == 2 || c->o.reuse_neg == 4)) {

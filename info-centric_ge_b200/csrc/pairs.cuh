@@ -657,213 +657,14 @@ __global__ void __launch_bounds__(256, 4) k_sgns_reuse_tile(SgArgs a) {
   if (lane == 0 && my_pairs) atomicAdd(a.pairs, my_pairs);
 }
 
-// -reuse-neg 3 (BF16 form): the center tile of -reuse-neg 2 scored on the
-// tensor cores.  Per center all n <= 32 context rows and the K + 1 target rows
-// are read at the start of the center and staged in shared memory as BF16 (FP32
-// master rows rounded to nearest); F = X Y^T comes from mma.sync m16n8k16
-// (BF16 in, FP32 accumulate; two 16-row tiles x DIM/16 k-steps).  A context
-// word that occurs twice in the window gets the sum of its rows of G, a
-// negative that occurs twice the sum of its columns, so every row receives one
-// update per center: syn0[c] += sum_j G_cj y_j (y in FP32), syn1[t_j] +=
-// sum_c G_cj x_c (x as staged).
+// Center tiles of -reuse-neg 3 hold at most kTileRows contexts per center
+// (window <= kTileRows / 2); their staging rounds to nearest BF16.
 constexpr int kTileRows = 32;
-constexpr int kTileWarps = 3;  // warps per block (the staging fits the 48-KB static shared memory)
-
-__device__ __forceinline__ void mma_bf16_16816(float (&d)[4], const uint32_t (&a)[4], const uint32_t (&b)[2]) {
-  asm volatile(
-      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
-      "{%0, %1, %2, %3};"
-      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
-}
 
 __device__ __forceinline__ uint32_t bf16x2_rn(float hi, float lo) {
   uint32_t d;
   asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(d) : "f"(hi), "f"(lo));
   return d;
-}
-
-template <int DIM, int NK>
-struct TileSmem {
-  static constexpr int kStride = DIM / 2 + 4;  // 32-bit words per staged row (DIM bf16 + 16 B): conflict-free fragments
-  uint32_t x[kTileRows][kStride];
-  uint32_t y[8][kStride];
-  float g[kTileRows][8];
-  int word[kTileRows];
-  int first[kTileRows];
-};
-
-template <int DIM, int NK>
-__global__ void __launch_bounds__(32 * kTileWarps) k_sgns_reuse_tile_tc(SgArgs a) {
-  static_assert(DIM == 64 || DIM == 128, "staged tile sizes");
-  constexpr int H = DIM / 64;       // float2 per lane per row
-  constexpr int W = DIM / 64;       // 32-bit bf16x2 words per lane per row (J = DIM / 32 values)
-  constexpr int NT = NK + 1;
-  static_assert(NT <= 8, "one 8-column tile");
-  using P = RowsBF16;
-  __shared__ float s_exp[1000];
-  __shared__ TileSmem<DIM, NK> sm_all[kTileWarps];
-  load_exp(a, s_exp);
-  TileSmem<DIM, NK> &sm = sm_all[threadIdx.x >> 5];
-  const int lane = lane_id();
-  const int gid = lane >> 2, tig = lane & 3;
-  LaneRows<DIM, P> rows;
-  rows.init(a);
-  unsigned long long my_pairs = 0;
-  unsigned long long s;
-  while (claim_sentence(a, s)) {
-    const long long sb = (long long)a.sent_start[s], se = (long long)a.sent_start[s + 1];
-    int neg[NK];
-#pragma unroll
-    for (int q = 0; q < NK; q++) neg[q] = __ldg(&a.negs[s * (uint64_t)NK + q]);
-    for (long long pos = sb; pos < se; pos++) {
-      const int word = __ldg(&a.sen[pos]);
-      long long c0 = pos - a.window, c1 = pos + a.window;
-      if (c0 < sb) c0 = sb;
-      if (c1 > se - 1) c1 = se - 1;
-      const int n = (int)(c1 - c0);  // contexts (the center excluded)
-      if (n < 1) continue;
-      int tg[NT];
-      tg[0] = word;
-#pragma unroll
-      for (int q = 0; q < NK; q++) tg[q + 1] = neg[q] == word ? -1 : neg[q];
-      // stage targets: FP32 values in registers, BF16 in shared memory
-      float2 y[NT][H];
-#pragma unroll
-      for (int q = 0; q < NT; q++) {
-#pragma unroll
-        for (int k = 0; k < H; k++) y[q][k] = make_float2(0.0f, 0.0f);
-        if (tg[q] >= 0) rows.template load<1>((uint32_t)tg[q], y[q]);
-#pragma unroll
-        for (int k = 0; k < W; k++) sm.y[q][lane * W + k] = bf16x2_rn(y[q][k].y, y[q][k].x);
-      }
-#pragma unroll
-      for (int q = NT; q < 8; q++)
-#pragma unroll
-        for (int k = 0; k < W; k++) sm.y[q][lane * W + k] = 0u;
-      // stage contexts in window order; rows past n are zero
-      for (int i = 0; i < kTileRows; i++) {
-        long long c = c0 + i;
-        if (c >= pos) c++;
-        const bool live = i < n;
-        const int w = live ? __ldg(&a.sen[c]) : 0;
-        float2 x[H];
-        if (live) rows.template load<0>((uint32_t)w, x);
-#pragma unroll
-        for (int k = 0; k < W; k++) sm.x[i][lane * W + k] = live ? bf16x2_rn(x[k].y, x[k].x) : 0u;
-        if (lane == 0) sm.word[i] = live ? w : -1;
-      }
-      __syncwarp();
-      // first occurrence of each context word in the window
-      {
-        int f = lane;
-        if (lane < n) {
-          const int w = sm.word[lane];
-          for (int j = 0; j < lane; j++)
-            if (sm.word[j] == w) {
-              f = j;
-              break;
-            }
-        }
-        sm.first[lane] = f;
-      }
-      // F = X Y^T on the tensor cores
-      float acc[2][4];
-#pragma unroll
-      for (int mt = 0; mt < 2; mt++)
-#pragma unroll
-        for (int r = 0; r < 4; r++) acc[mt][r] = 0.0f;
-#pragma unroll
-      for (int kk = 0; kk < DIM / 16; kk++) {
-        const int col = kk * 8 + tig;  // 32-bit word of the k-step (2 bf16 per word)
-        uint32_t b[2] = {sm.y[gid][col], sm.y[gid][col + 4]};
-#pragma unroll
-        for (int mt = 0; mt < 2; mt++) {
-          const int r0 = mt * 16 + gid;
-          uint32_t af[4] = {sm.x[r0][col], sm.x[r0 + 8][col], sm.x[r0][col + 4], sm.x[r0 + 8][col + 4]};
-          mma_bf16_16816(acc[mt], af, b);
-        }
-      }
-      // G = (label - sigma(F)) alpha on valid (context, target) cells
-      uint32_t vmask = 0;
-#pragma unroll
-      for (int q = 0; q < NT; q++) vmask |= (tg[q] >= 0 ? 1u : 0u) << q;
-#pragma unroll
-      for (int mt = 0; mt < 2; mt++)
-#pragma unroll
-        for (int r = 0; r < 4; r++) {
-          const int row = mt * 16 + gid + (r >= 2 ? 8 : 0);
-          const int colj = tig * 2 + (r & 1);
-          const bool ok = row < n && colj < NT && ((vmask >> colj) & 1u);
-          sm.g[row][colj] = ok ? sg_grad(acc[mt][r], colj == 0 ? 1 : 0, s_exp, a.alpha) : 0.0f;
-        }
-      __syncwarp();
-      // merge the rows of repeated context words into their first occurrence
-      if (lane < 8) {
-        for (int i = 1; i < n; i++) {
-          const int f = sm.first[i];
-          if (f != i) {
-            sm.g[f][lane] = __fadd_rn(sm.g[f][lane], sm.g[i][lane]);
-            sm.g[i][lane] = 0.0f;
-          }
-        }
-      }
-      __syncwarp();
-      const uint32_t center = (uint32_t)(pos - sb);
-      const uint32_t key = lane_mix(pair_key(a.sr_seed, s, center), lane);
-      float2 dy[NT][H];
-#pragma unroll
-      for (int q = 0; q < NT; q++)
-#pragma unroll
-        for (int k = 0; k < H; k++) dy[q][k] = make_float2(0.0f, 0.0f);
-      for (int i = 0; i < n; i++) {
-        // staged context values (x as the tile saw it)
-        float2 xs[H];
-#pragma unroll
-        for (int k = 0; k < W; k++) {
-          const uint32_t w2 = sm.x[i][lane * W + k];
-          xs[k] = make_float2(bf16_lo(w2), bf16_hi(w2));
-        }
-        float2 neu[H];
-#pragma unroll
-        for (int k = 0; k < H; k++) neu[k] = make_float2(0.0f, 0.0f);
-#pragma unroll
-        for (int q = 0; q < NT; q++) {
-          const float g = sm.g[i][q];
-          const float2 g2 = make_float2(g, g);
-#pragma unroll
-          for (int k = 0; k < H; k++) {
-            neu[k] = __ffma2_rn(g2, y[q][k], neu[k]);
-            dy[q][k] = __ffma2_rn(g2, xs[k], dy[q][k]);
-          }
-        }
-        if (sm.first[i] == i) {
-          const uint32_t w = (uint32_t)sm.word[i];
-          const long long c = c0 + i + (c0 + i >= pos ? 1 : 0);
-          rows.template update<0>(w, neu, xs, key, kSlotCtx + (uint32_t)(c - pos + a.window));
-        }
-        my_pairs++;
-      }
-      // targets: a repeated negative adds its sum into the first occurrence
-#pragma unroll
-      for (int q = 2; q < NT; q++) {
-        bool merged = false;
-#pragma unroll
-        for (int r = 1; r < q; r++) {
-          const bool hit = !merged && tg[q] >= 0 && tg[r] == tg[q];
-#pragma unroll
-          for (int k = 0; k < H; k++) dy[r][k] = hit ? __fadd2_rn(dy[r][k], dy[q][k]) : dy[r][k];
-          merged |= hit;
-        }
-        if (merged) tg[q] = -2;
-      }
-#pragma unroll
-      for (int q = 0; q < NT; q++)
-        if (tg[q] >= 0) rows.template update<1>((uint32_t)tg[q], dy[q], y[q], key, (uint32_t)q);
-      __syncwarp();
-    }
-  }
-  if (lane == 0 && my_pairs) atomicAdd(a.pairs, my_pairs);
 }
 
 // Row references of a chunk of pair records: per pair its context row and

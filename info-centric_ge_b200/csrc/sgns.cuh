@@ -92,6 +92,7 @@ struct SgArgs {
   const uint32_t *coarse;
   FastMod fm_table;
   const unsigned long long *jump_a, *jump_c;
+  int *err;  // device error code (bounded waits that give up)
 };
 
 // ------------------------------------------------------------ row access

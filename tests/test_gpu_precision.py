@@ -179,7 +179,7 @@ def test_window_tile_deterministic_matches_oracle(precision, dim, negative, wind
 
 @pytest.mark.parametrize("dim,negative", [(128, 5), (64, 7)])
 def test_reuse_tile_tensor_core_matches_oracle(dim, negative):
-    """-reuse-neg 3 (BF16 form, center tiles scored by mma.sync bf16) in the
+    """-reuse-neg 3 (BF16 form, center tiles scored by tcgen05.mma BF16) in the
     one-warp mode against the oracle's restatement with FP64 dots of the same
     BF16 operands.  The tensor core's FP32 accumulation order is unspecified,
     so a score can differ in its last bits and flip a stochastic rounding that
