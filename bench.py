@@ -96,7 +96,10 @@ FORMS = {
 }
 BUDGET_MODEL = os.path.join(ROOT, "info-centric_ge_b200", "felog_b200", "budget_mlp_c4.npy")
 METRIC = "walk+SGNS corpus tokens/s (walk steps/s and SGNS words/s reported alongside)"
-WALK_BYTES_PER_STEP = 68      # 2 random 32-B sectors + 4-B token write
+# algorithmic bytes of a walk step in the sector model of the reference's CSR:
+# the candidate's adjacency sector, its row_ptr sector, the 4-B token; with the
+# walker entries a step reads one 32-B sector, which walk_kernel.layout states
+WALK_BYTES_PER_STEP = 68
 # DRAM bytes per pair of k_sgns_train_pairs<128, 5> (dram__bytes_read.sum + dram__bytes_write.sum of one ncu
 # capture of the profiling case's timed round divided by its 66.0 M pairs), scaled to a launch
 DRAM_BYTES_PER_PAIR = {"fp32": 1055.6, "bf16": 244.1}  # bf16: 5 blocks per SM; fp32: 4
@@ -357,6 +360,15 @@ def reference_quality(g, pairs):
             "wall_s": time.perf_counter() - t0}
 
 
+def walk_layout(f):
+    wb = f.walk_entries()
+    if wb:
+        return {"walker_entries_bytes": wb, "dram_sectors_per_step": 1,
+                "what": "walker entries (16 B: neighbour, data, its first entry and degree): one dependent random "
+                        "read per step; bytes_per_step stays the sector model of the reference's CSR"}
+    return {"walker_entries_bytes": 0, "dram_sectors_per_step": 2, "what": "plain CSR: two dependent random reads"}
+
+
 FORM_SET = ("plain-fp32", "learned-bf16", "learned-bf16-window", "learned-bf16-tile", "learned-fp32-tile")
 
 
@@ -560,6 +572,7 @@ def bench_mine(args):
                      "peak_source": peak_kind,
                      "walk_kernel": {"achieved": walk_achieved, "frac": walk_achieved / peak,
                                      "bytes_per_step": WALK_BYTES_PER_STEP,
+                                     "layout": walk_layout(f),
                                      "gather_ceiling": {"steps_per_s": ceil_tok / (ceil_ms * 1e-3),
                                                         "walk_steps_per_s": last_tok / (last_ms * 1e-3),
                                                         "frac": (last_tok / last_ms) / (ceil_tok / ceil_ms),
@@ -670,6 +683,7 @@ def bench_streamed(args):
             cpu = cpu_baseline_resident(f, V)
         except Exception as ex:  # reported, not fatal
             cpu = {"error": str(ex)}
+    layout = walk_layout(f)
     f.close()
     out = {
         "metric": METRIC, "value": cnt["tokens"] / (ms * 1e-3), "unit": "tokens/s", "n_gpus": 1,
@@ -697,7 +711,7 @@ def bench_streamed(args):
                      "algorithmic_bytes_per_pair": refs_per_pair * per_ref, "row_refs_per_pair": refs_per_pair,
                      "master_row_share": hot_share, "peak_source": peak_kind,
                      "walk_kernel": {"achieved": walk_achieved, "frac": walk_achieved / peak,
-                                     "bytes_per_step": WALK_BYTES_PER_STEP}},
+                                     "bytes_per_step": WALK_BYTES_PER_STEP, "layout": layout}},
         "e2e": {"value": job["walk_tokens"] / e2e_s, "unit": "tokens/s", "h2d_bytes_per_step": 120,
                 "d2h_bytes_per_step": int(vs * TRAIN["size"] * 4),
                 "what": "one whole job per step: device generation from the parameter block, felog_run to the "

@@ -287,6 +287,14 @@ felog_status felog_get_visit_freq(felog_ctx *ctx, uint64_t *freq);
  * device (best of 3).  ms: its duration; tokens: the tokens it emits.  The
  * corpus is left unchanged. */
 felog_status felog_walk_ceiling(felog_ctx *ctx, float *ms, uint64_t *tokens);
+/* Walker entries (no counterpart in the reference, whose walker reads its CSR,
+ * graph.hpp:531-575): next to the CSR, the library keeps every entry as 16
+ * bytes {neighbour, data, the neighbour's first entry, its degree}, so a walk
+ * step makes one dependent random read instead of two.  They are built by
+ * load_graph / load_rmat for graphs of at most 2^31 CSR entries when the
+ * device has room, and the walker and felog_walk_ceiling use them then.
+ * bytes: their device size, 0 when the walker reads the plain CSR. */
+felog_status felog_walk_entries(felog_ctx *ctx, uint64_t *bytes);
 
 /* ---- offline edge data ---- */
 /* Common neighbours per input edge: the reference's offline tool

@@ -91,6 +91,7 @@ struct felog_ctx {
   uint64_t M = 0;
   DevBuf<uint64_t> row_ptr;
   DevBuf<uint2> adj;
+  DevBuf<uint4> wadj;  // walker entries (k_fuse_adj); empty above kFuseMaxEntries or without room
   DevBuf<uint32_t> deg;
   std::vector<uint32_t> h_deg;
   DevBuf<float> alias_prob;
@@ -388,7 +389,7 @@ extern "C" void felog_destroy(felog_ctx *c) {
   c->copy_stage.release();
   if (c->stream) cudaStreamSynchronize(c->stream);
   if (c->mbox) cudaFreeHost(c->mbox);
-  c->row_ptr.release(); c->adj.release(); c->deg.release(); c->alias_prob.release(); c->alias_idx.release();
+  c->row_ptr.release(); c->adj.release(); c->wadj.release(); c->deg.release(); c->alias_prob.release(); c->alias_idx.release();
   c->stop.release(); c->active.release(); c->arena.release(); c->sent_ptr.release(); c->sent_len.release();
   c->visit_freq.release(); c->counters.release(); c->derr.release(); c->inj_idx_off.release();
   c->inj_p_off.release(); c->inj_idx.release(); c->inj_p.release(); c->flags_tmp.release();
@@ -410,6 +411,8 @@ extern "C" const char *felog_last_error(const felog_ctx *c) { return c ? c->err.
 // ----------------------------------------------------------------- graph
 
 namespace {
+
+constexpr uint64_t kFuseMaxEntries = 1ull << 31;
 
 // CSR of n device records (3 words each: src, dst, data bits), doubled when
 // undirected; the records stay the caller's.  Entry indices are 32-bit, so at
@@ -461,6 +464,19 @@ felog_status build_csr(felog_ctx *c, const uint32_t *rec, uint64_t n, uint32_t v
   CK(cudaStreamSynchronize(c->stream), "load_graph");
   keys.release(); vals.release(); keys2.release(); vals2.release();
   c->cub_tmp.release();
+  // walker entries, while they take at most 32 GB (2^31 entries); without
+  // room for them the walk reads the plain CSR
+  c->wadj.release();
+  if (m && m <= kFuseMaxEntries) {
+    if (c->wadj.ensure(m) == cudaSuccess) {
+      k_fuse_adj<<<grid_for(c, m, 256), 256, 0, c->stream>>>(c->row_ptr.p, c->adj.p, m, c->wadj.p);
+      c->launches++;
+      CK(cudaGetLastError(), "load_graph: walker entries");
+    } else {
+      cudaGetLastError();
+      c->wadj.release();
+    }
+  }
   c->V = v_num;
   c->M = m;
   c->has_alias = false;
@@ -876,6 +892,7 @@ felog_status walk_range(felog_ctx *c, uint32_t round, const felog_draws *draws, 
   WalkArgs a{};
   a.row_ptr = c->row_ptr.p;
   a.adj = c->adj.p;
+  a.wadj = c->wadj.p;
   a.alias_prob = c->alias_prob.p;
   a.alias_idx = c->alias_idx.p;
   a.v_num = c->V;
@@ -909,7 +926,9 @@ felog_status walk_range(felog_ctx *c, uint32_t round, const felog_draws *draws, 
   if (na) {
     // persistent grid: exactly the blocks that are resident at once, so no
     // block waits for a slot only to find every walker claimed
-    void (*kern)(WalkArgs) = a.injected ? k_walk<true, false> : a.weighted ? k_walk<false, true> : k_walk<false, false>;
+    void (*kern)(WalkArgs);
+    if (a.wadj) kern = a.injected ? k_walk<true, false, true> : a.weighted ? k_walk<false, true, true> : k_walk<false, false, true>;
+    else kern = a.injected ? k_walk<true, false, false> : a.weighted ? k_walk<false, true, false> : k_walk<false, false, false>;
     int per_sm = 0;
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kWalkThreads, 0), "walk_round: occupancy");
     const int blocks = c->sm_count * std::max(per_sm, 1);
@@ -1004,13 +1023,17 @@ felog_status walk_ceiling_run(felog_ctx *c, DevBuf<uint32_t> &scratch, float *ms
   CK(scratch.ensure(c->arena_cap), "walk_ceiling: scratch");
   CK(c->walk_claim.ensure(1), "walk_ceiling");
   int per_sm = 0;
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_walk_skeleton, kWalkThreads, 0), "walk_ceiling");
+  const bool fused = c->wadj.p != nullptr;
+  void (*skel)(const uint64_t *, const uint2 *, const uint4 *, uint32_t, uint32_t, const uint32_t *, const uint64_t *,
+               const uint32_t *, uint32_t, uint32_t *, unsigned int *) =
+      fused ? k_walk_skeleton<true> : k_walk_skeleton<false>;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, skel, kWalkThreads, 0), "walk_ceiling");
   const int blocks = c->sm_count * std::max(per_sm, 1);
   float best = 0;
   for (int rep = 0; rep < 3; rep++) {
     CK(cudaMemsetAsync(c->walk_claim.p, 0, 4, c->stream), "walk_ceiling");
     CK(cudaEventRecord(c->ev0, c->stream), "walk_ceiling");
-    k_walk_skeleton<<<blocks, kWalkThreads, 0, c->stream>>>(c->row_ptr.p, c->adj.p, c->V, (uint32_t)c->n_sent,
+    skel<<<blocks, kWalkThreads, 0, c->stream>>>(c->row_ptr.p, c->adj.p, c->wadj.p, c->V, (uint32_t)c->n_sent,
                                                              c->active.p + c->chunk_base, c->sent_ptr.p, c->sent_len.p,
                                                              frac, scratch.p, c->walk_claim.p);
     c->launches++;
@@ -1025,6 +1048,12 @@ felog_status walk_ceiling_run(felog_ctx *c, DevBuf<uint32_t> &scratch, float *ms
   return FELOG_OK;
 }
 }  // namespace
+
+extern "C" felog_status felog_walk_entries(felog_ctx *c, uint64_t *bytes) {
+  if (!c || !bytes) return FELOG_INVALID_ARG;
+  *bytes = c->wadj.p ? (uint64_t)c->M * sizeof(uint4) : 0;
+  return FELOG_OK;
+}
 
 extern "C" felog_status felog_walk_ceiling(felog_ctx *c, float *ms, uint64_t *tokens) {
   if (!c || !ms) return FELOG_INVALID_ARG;

@@ -34,6 +34,20 @@ __global__ void k_expand_edges(const uint32_t *__restrict__ rec /* 3 words per r
   }
 }
 
+// Walker entries: wadj[j] = {neighbour, data bits, the neighbour's first CSR
+// entry, its degree}.  A walk step reads its candidate's entry and, from the
+// same 16 bytes, where the candidate's own list starts and how long it is, so
+// a step costs one dependent random read instead of two (adj[b + r], then
+// row_ptr[dst], row_ptr[dst + 1]).  Entry indices are below 2^32.
+__global__ void k_fuse_adj(const uint64_t *__restrict__ row_ptr, const uint2 *__restrict__ adj, uint64_t m,
+                           uint4 *__restrict__ wadj) {
+  for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < m; j += (uint64_t)gridDim.x * blockDim.x) {
+    const uint2 e = adj[j];
+    const uint64_t b = row_ptr[e.x];
+    wadj[j] = make_uint4(e.x, e.y, (uint32_t)b, (uint32_t)(row_ptr[e.x + 1] - b));
+  }
+}
+
 // Gather entries into CSR order: adj[j] = {neighbour, data bits}.
 __global__ void k_gather_adj(const uint32_t *__restrict__ rec, const uint32_t *__restrict__ order, uint64_t m,
                              int undirected, uint2 *__restrict__ adj) {

@@ -43,6 +43,7 @@ namespace felog {
 struct WalkArgs {
   const uint64_t *row_ptr;
   const uint2 *adj;
+  const uint4 *wadj;        // walker entries {neighbour, data, its row start, its degree} (k_fuse_adj), or NULL
   const float *alias_prob;  // weighted mode only
   const uint32_t *alias_idx;
   uint32_t v_num;
@@ -243,8 +244,10 @@ __device__ __forceinline__ bool path_push(const WalkArgs &a, PathBuf &pb, uint32
   return true;
 }
 
-// INJ: parity mode with injected draws; WEIGHTED: alias-table candidates.
-template <bool INJ, bool WEIGHTED>
+// INJ: parity mode with injected draws; WEIGHTED: alias-table candidates;
+// FUSED: candidates read from the walker entries (one dependent random read
+// per step; the walk is the same).
+template <bool INJ, bool WEIGHTED, bool FUSED>
 __global__ void __launch_bounds__(kWalkThreads, 3) k_walk(WalkArgs a) {
   __shared__ uint32_t s_path[kSmemPath * kWalkThreads];
   __shared__ double4 s_ser[kCorrSeries];
@@ -310,8 +313,18 @@ __global__ void __launch_bounds__(kWalkThreads, 3) k_walk(WalkArgs a) {
         set_error(a.err, kErrWalkLimit);
         break;
       }
-      if (deg == 2 && a.adj[b].x == cur) break;
-      const uint2 cand = a.adj[b + r];
+      if (deg == 2 && (FUSED ? a.wadj[b].x : a.adj[b].x) == cur) break;
+      uint2 cand;
+      uint64_t bd;
+      uint32_t dd;
+      if constexpr (FUSED) {
+        const uint4 e = a.wadj[b + r];
+        cand = make_uint2(e.x, e.y);
+        bd = e.z;
+        dd = e.w;
+      } else {
+        cand = a.adj[b + r];
+      }
       if (step == 0 && cand.x == cur) continue;
       if (INJ) {
         if (dp >= dp_end) {
@@ -322,8 +335,10 @@ __global__ void __launch_bounds__(kWalkThreads, 3) k_walk(WalkArgs a) {
       }
       const int cn = (int)__uint_as_float(cand.y);
       const uint32_t dst = cand.x;
-      const uint64_t bd = a.row_ptr[dst];
-      const uint32_t dd = (uint32_t)(a.row_ptr[dst + 1] - bd);
+      if constexpr (!FUSED) {
+        bd = a.row_ptr[dst];
+        dd = (uint32_t)(a.row_ptr[dst + 1] - bd);
+      }
       const int sd = (int)deg, ddi = (int)dd;
       const int mx = sd > ddi ? sd : ddi, mn = sd < ddi ? sd : ddi;
       const bool trace = trace_test(sd, cn, mx, mn, p);
@@ -375,15 +390,18 @@ __global__ void __launch_bounds__(kWalkThreads, 3) k_walk(WalkArgs a) {
 // Memory skeleton of a finished walk round, for its attainable-rate ceiling:
 // every walker of the round emits as many tokens as its walk had; a token is
 // a dependent uniform-neighbour gather (the candidate's adjacency entry, then
-// the neighbour's row_ptr pair) with probability gather_frac (the round's
+// the neighbour's row_ptr pair; with FUSED the candidate's walker entry alone,
+// as the walker reads it) with probability gather_frac (the round's
 // forward steps per token), else a repeat of the current vertex (the return
 // token of a trace, which loads nothing).  Same block size and warp claims
 // as k_walk, at its own full residency (no shared memory and few registers
 // give 8 blocks per SM, where k_walk holds 3); no FP64, no trace test, no
 // revisit counts and no visit counters.  Tokens go to a scratch buffer at
 // the walk's offsets.
+template <bool FUSED>
 __global__ void __launch_bounds__(kWalkThreads, 3)
-    k_walk_skeleton(const uint64_t *__restrict__ row_ptr, const uint2 *__restrict__ adj, uint32_t v_num,
+    k_walk_skeleton(const uint64_t *__restrict__ row_ptr, const uint2 *__restrict__ adj,
+                    const uint4 *__restrict__ wadj, uint32_t v_num,
                     uint32_t n_active, const uint32_t *__restrict__ active, const uint64_t *__restrict__ sent_ptr,
                     const uint32_t *__restrict__ sent_len, uint32_t gather_frac, uint32_t *out,
                     unsigned int *next_walker) {
@@ -407,10 +425,17 @@ __global__ void __launch_bounds__(kWalkThreads, 3)
       h = h * 1664525u + 1013904223u;
       if (deg && (h >> 8) < (gather_frac >> 8)) {
         const uint32_t r = (uint32_t)(((uint64_t)(h ^ (h >> 13)) * deg) >> 32);
-        const uint32_t dst = adj[b + r].x;
-        b = row_ptr[dst];
-        deg = (uint32_t)(row_ptr[dst + 1] - b);
-        cur = dst;
+        if constexpr (FUSED) {
+          const uint4 e = wadj[b + r];
+          cur = e.x;
+          b = e.z;
+          deg = e.w;
+        } else {
+          const uint32_t dst = adj[b + r].x;
+          b = row_ptr[dst];
+          deg = (uint32_t)(row_ptr[dst + 1] - b);
+          cur = dst;
+        }
       }
       o[t] = cur;
     }

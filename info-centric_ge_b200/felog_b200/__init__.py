@@ -158,6 +158,7 @@ def gpu_lib():
         L.felog_set_corpus.argtypes = [_P, _P, _P, ctypes.c_uint64]
         L.felog_get_visit_freq.argtypes = [_P, _P]
         L.felog_walk_ceiling.argtypes = [_P, _P, _P]
+        L.felog_walk_entries.argtypes = [_P, _P]
         L.felog_pair_row_mix.argtypes = [_P, _P, _P, _P]
         L.felog_format_lf.argtypes = [_P, ctypes.c_uint64, _P, ctypes.c_uint64, _P]
         L.felog_common_neighbours.argtypes = [_P, _P, _P, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_int, _P, _P]
@@ -365,6 +366,13 @@ class Felog:
         v = [ctypes.c_uint64() for _ in range(3)]
         self._ck(self._L.felog_pair_row_mix(self.h, *[ctypes.byref(x) for x in v]))
         return tuple(x.value for x in v)
+
+    def walk_entries(self):
+        """Device bytes of the walker entries (felog_walk_entries); 0 when the
+        walker reads the plain CSR."""
+        b = ctypes.c_uint64()
+        self._ck(self._L.felog_walk_entries(self.h, ctypes.byref(b)))
+        return b.value
 
     def walk_ceiling(self):
         """Memory skeleton of the last walk round (felog_walk_ceiling):
