@@ -1339,6 +1339,26 @@ __global__ void k_unigram_fill(const double *__restrict__ cum, uint64_t n, uint6
     table[a] = (int32_t)lo;
   }
 }
+// The reference's table (word2vec.cu:674-694) walks the slots in order and
+// moves to the next word at most once per slot, when a / T > d1, d1 being the
+// running FP64 sum of the words' shares.  With D(k) that sum through word k
+// (the same sequential FP64 sum) and firstA(k) the first slot with
+// a / T > D(k), the first slot of word k + 1 is max(start(k), firstA(k)) + 1,
+// so start(k) = k + max(0, max_{j<k} (firstA(j) - j)): a prefix maximum the
+// host takes in one pass.  Slot a then holds the last word whose start is
+// <= a (the last word once the walk passes it, as the reference clamps).
+__global__ void k_unigram_fill_starts(const uint64_t *__restrict__ start, uint64_t n, uint64_t T,
+                                      int32_t *__restrict__ table) {
+  for (uint64_t a = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; a < T; a += (uint64_t)gridDim.x * blockDim.x) {
+    uint64_t lo = 0, hi = n - 1;  // last k with start[k] <= a (start[0] = 0)
+    while (lo < hi) {
+      const uint64_t mid = (lo + hi + 1) >> 1;
+      if (start[mid] <= a) lo = mid;
+      else hi = mid - 1;
+    }
+    table[a] = (int32_t)lo;
+  }
+}
 }  // namespace
 
 extern "C" felog_status felog_init_model(felog_ctx *c) {
@@ -1389,23 +1409,37 @@ extern "C" felog_status felog_init_model(felog_ctx *c) {
   CK(c->id2offset.ensure(V), "init_model");
   CK(cudaMemcpy(c->id2offset.p, c->h_id2offset.data(), 4 * (size_t)V, cudaMemcpyHostToDevice), "init_model");
   if (size <= kRefTableMaxVocab) {
-    // unigram table (word2vec.cu:674-694): the reference's 1e8 slots, sequential FP64 walk
-    std::vector<int32_t> table(kTableSize);
-    double twp = 0, d1, power = 0.75;
-    long long i = 0;
-    for (long long a = 0; a < size; a++) twp += pow((double)cn[a], power);
-    d1 = pow((double)cn[0], power) / twp;
-    for (int64_t a = 0; a < kTableSize; a++) {
-      table[a] = (int32_t)i;
-      if (a / (double)kTableSize > d1) {
-        i++;
-        d1 += pow((double)cn[i < size ? i : size - 1], power) / twp;
-      }
-      if (i >= size) i = size - 1;
+    // unigram table (word2vec.cu:674-694): the reference's 1e8 slots and FP64
+    // sums; the first slot of every word on the host (k_unigram_fill_starts
+    // has the argument), the slots on the device
+    const double power = 0.75, T = (double)kTableSize;
+    std::vector<double> w(size);
+    for (long long a = 0; a < size; a++) w[a] = (a > 0 && cn[a] == cn[a - 1]) ? w[a - 1] : pow((double)cn[a], power);
+    double twp = 0;
+    for (long long a = 0; a < size; a++) twp += w[a];
+    std::vector<uint64_t> start(size);
+    double d1 = w[0] / twp;
+    long long run = 0;  // max_{j<k} (firstA(j) - j), or 0
+    for (long long k = 0; k < size; k++) {
+      if (k > 0) d1 += w[k] / twp;
+      start[k] = (uint64_t)(k + run);
+      // firstA(k): the first slot a with a / T > d1
+      long long fa = (long long)std::floor(d1 * T);
+      if (fa < 0) fa = 0;
+      while (fa > 0 && (double)(fa - 1) / T > d1) fa--;
+      while (!((double)fa / T > d1)) fa++;
+      run = std::max(run, fa - k);
     }
     c->table_size = kTableSize;
     CK(c->table.ensure(kTableSize), "init_model: unigram table");
-    CK(cudaMemcpy(c->table.p, table.data(), 4 * (size_t)kTableSize, cudaMemcpyHostToDevice), "init_model");
+    DevBuf<uint64_t> dstart;
+    CK(dstart.ensure(size), "init_model: unigram table");
+    CK(cudaMemcpyAsync(dstart.p, start.data(), 8 * (size_t)size, cudaMemcpyHostToDevice, c->stream), "init_model");
+    k_unigram_fill_starts<<<grid_for(c, kTableSize, 256), 256, 0, c->stream>>>(dstart.p, (uint64_t)size, kTableSize,
+                                                                              c->table.p);
+    c->launches++;
+    CK(cudaGetLastError(), "init_model: unigram table");
+    CK(cudaStreamSynchronize(c->stream), "init_model");
   } else {
     // larger vocabularies: 1e8 slots would leave most words without a slot, so
     // the table has the power of two >= 8 x vocabulary slots, slot a holding
