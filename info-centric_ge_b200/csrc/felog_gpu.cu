@@ -1417,18 +1417,27 @@ extern "C" felog_status felog_init_model(felog_ctx *c) {
     for (long long a = 0; a < size; a++) w[a] = (a > 0 && cn[a] == cn[a - 1]) ? w[a - 1] : pow((double)cn[a], power);
     double twp = 0;
     for (long long a = 0; a < size; a++) twp += w[a];
-    std::vector<uint64_t> start(size);
+    // D(k) in the reference's order, then firstA(k) per word (independent,
+    // on all host threads), then the prefix maximum
+    std::vector<double> dsum(size);
     double d1 = w[0] / twp;
+    dsum[0] = d1;
+    for (long long k = 1; k < size; k++) dsum[k] = d1 += w[k] / twp;
+    std::vector<long long> fa(size);
+#pragma omp parallel for schedule(static)
+    for (long long k = 0; k < size; k++) {
+      // firstA(k): the first slot a with a / T > D(k)
+      long long x = (long long)std::floor(dsum[k] * T);
+      if (x < 0) x = 0;
+      while (x > 0 && (double)(x - 1) / T > dsum[k]) x--;
+      while (!((double)x / T > dsum[k])) x++;
+      fa[k] = x;
+    }
+    std::vector<uint64_t> start(size);
     long long run = 0;  // max_{j<k} (firstA(j) - j), or 0
     for (long long k = 0; k < size; k++) {
-      if (k > 0) d1 += w[k] / twp;
       start[k] = (uint64_t)(k + run);
-      // firstA(k): the first slot a with a / T > d1
-      long long fa = (long long)std::floor(d1 * T);
-      if (fa < 0) fa = 0;
-      while (fa > 0 && (double)(fa - 1) / T > d1) fa--;
-      while (!((double)fa / T > d1)) fa++;
-      run = std::max(run, fa - k);
+      run = std::max(run, fa[k] - k);
     }
     c->table_size = kTableSize;
     CK(c->table.ensure(kTableSize), "init_model: unigram table");
@@ -1473,6 +1482,7 @@ extern "C" felog_status felog_init_model(felog_ctx *c) {
       double stw = sample * (double)tw;
       if (stw > 0.0) {
         thr.assign(size, 65535);
+#pragma omp parallel for schedule(static)
         for (long long i = 0; i < size; i++) {
           long long count = cn[i];
           if (count <= 0) continue;
