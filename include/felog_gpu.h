@@ -293,8 +293,10 @@ felog_status felog_walk_ceiling(felog_ctx *ctx, float *ms, uint64_t *tokens);
  * step makes one dependent random read instead of two.  They are built by
  * load_graph / load_rmat for graphs of at most 2^31 CSR entries when the
  * device has room, and the walker and felog_walk_ceiling use them then.
- * bytes: their device size, 0 when the walker reads the plain CSR. */
-felog_status felog_walk_entries(felog_ctx *ctx, uint64_t *bytes);
+ * keep = 0 frees them (the walker reads the plain CSR from then on, until the
+ * next graph load); bytes (may be NULL): their device size afterwards, 0 when
+ * the walker reads the plain CSR. */
+felog_status felog_walk_entries(felog_ctx *ctx, int keep, uint64_t *bytes);
 
 /* ---- offline edge data ---- */
 /* Common neighbours per input edge: the reference's offline tool

@@ -1049,9 +1049,14 @@ felog_status walk_ceiling_run(felog_ctx *c, DevBuf<uint32_t> &scratch, float *ms
 }
 }  // namespace
 
-extern "C" felog_status felog_walk_entries(felog_ctx *c, uint64_t *bytes) {
-  if (!c || !bytes) return FELOG_INVALID_ARG;
-  *bytes = c->wadj.p ? (uint64_t)c->M * sizeof(uint4) : 0;
+extern "C" felog_status felog_walk_entries(felog_ctx *c, int keep, uint64_t *bytes) {
+  if (!c) return FELOG_INVALID_ARG;
+  if (!keep && c->wadj.p) {
+    CK(cudaSetDevice(c->device), "walk_entries");
+    CK(cudaStreamSynchronize(c->stream), "walk_entries");
+    c->wadj.release();
+  }
+  if (bytes) *bytes = c->wadj.p ? (uint64_t)c->M * sizeof(uint4) : 0;
   return FELOG_OK;
 }
 

@@ -158,7 +158,7 @@ def gpu_lib():
         L.felog_set_corpus.argtypes = [_P, _P, _P, ctypes.c_uint64]
         L.felog_get_visit_freq.argtypes = [_P, _P]
         L.felog_walk_ceiling.argtypes = [_P, _P, _P]
-        L.felog_walk_entries.argtypes = [_P, _P]
+        L.felog_walk_entries.argtypes = [_P, ctypes.c_int, _P]
         L.felog_pair_row_mix.argtypes = [_P, _P, _P, _P]
         L.felog_format_lf.argtypes = [_P, ctypes.c_uint64, _P, ctypes.c_uint64, _P]
         L.felog_common_neighbours.argtypes = [_P, _P, _P, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_int, _P, _P]
@@ -367,11 +367,11 @@ class Felog:
         self._ck(self._L.felog_pair_row_mix(self.h, *[ctypes.byref(x) for x in v]))
         return tuple(x.value for x in v)
 
-    def walk_entries(self):
+    def walk_entries(self, keep=True):
         """Device bytes of the walker entries (felog_walk_entries); 0 when the
-        walker reads the plain CSR."""
+        walker reads the plain CSR.  keep=False frees them first."""
         b = ctypes.c_uint64()
-        self._ck(self._L.felog_walk_entries(self.h, ctypes.byref(b)))
+        self._ck(self._L.felog_walk_entries(self.h, 1 if keep else 0, ctypes.byref(b)))
         return b.value
 
     def walk_ceiling(self):

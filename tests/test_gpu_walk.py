@@ -41,10 +41,18 @@ def test_csr_matches_oracle(name):
     np.testing.assert_array_equal(f.degrees(), c.deg)
 
 
+@pytest.mark.parametrize("layout", ["entries", "csr"])
 @pytest.mark.parametrize("name", WALKS)
-def test_walk_injected_bit_exact_to_reference(name):
+def test_walk_injected_bit_exact_to_reference(name, layout):
+    """Both walker layouts: the walker entries (the default) and the plain CSR
+    (after felog_walk_entries frees the entries, as for graphs above 2^31
+    entries)."""
     fx = load_golden(name)
     f = ctx_for(fx)
+    if layout == "csr":
+        assert f.walk_entries(keep=False) == 0
+    else:
+        assert f.walk_entries() == 16 * len(f.csr()[1])
     for r in range(int(fx["rounds"])):
         st = f.walk_round(r, draws=walk_draws(fx, r))
         tok, off = f.corpus()
@@ -55,9 +63,12 @@ def test_walk_injected_bit_exact_to_reference(name):
 
 @pytest.mark.parametrize("name,rounds,slot", [("walk_rmat4096.npz", 3, 64), ("walk_edgecases.npz", 3, 64),
                                               ("walk_rmat512_stop_w2.npz", 2, 8), ("walk_rmat512.npz", 2, 4)])
-def test_walk_philox_bit_exact_to_oracle(name, rounds, slot):
+@pytest.mark.parametrize("layout", ["entries", "csr"])
+def test_walk_philox_bit_exact_to_oracle(name, rounds, slot, layout):
     fx = load_golden(name)
     f = ctx_for(fx, seed=1234, slot_len=slot)
+    if layout == "csr":
+        f.walk_entries(keep=False)
     V = int(fx["V"])
     c = ob.OracleCsr(fx["edges"], V)
     for r in range(rounds):
