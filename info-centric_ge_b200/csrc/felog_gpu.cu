@@ -413,6 +413,9 @@ extern "C" const char *felog_last_error(const felog_ctx *c) { return c ? c->err.
 namespace {
 
 constexpr uint64_t kFuseMaxEntries = 1ull << 31;
+// host threads for init_model's per-word loops: a few, so that a busy shared
+// host does not hold a parallel region up on a descheduled thread
+#define FELOG_INIT_THREADS 8
 
 // CSR of n device records (3 words each: src, dst, data bits), doubled when
 // undirected; the records stay the caller's.  Entry indices are 32-bit, so at
@@ -1429,7 +1432,7 @@ extern "C" felog_status felog_init_model(felog_ctx *c) {
     dsum[0] = d1;
     for (long long k = 1; k < size; k++) dsum[k] = d1 += w[k] / twp;
     std::vector<long long> fa(size);
-#pragma omp parallel for schedule(static)
+#pragma omp parallel for schedule(static) num_threads(FELOG_INIT_THREADS) if (size > 65536)
     for (long long k = 0; k < size; k++) {
       // firstA(k): the first slot a with a / T > D(k)
       long long x = (long long)std::floor(dsum[k] * T);
@@ -1487,7 +1490,7 @@ extern "C" felog_status felog_init_model(felog_ctx *c) {
       double stw = sample * (double)tw;
       if (stw > 0.0) {
         thr.assign(size, 65535);
-#pragma omp parallel for schedule(static)
+#pragma omp parallel for schedule(static) num_threads(FELOG_INIT_THREADS) if (size > 65536)
         for (long long i = 0; i < size; i++) {
           long long count = cn[i];
           if (count <= 0) continue;
