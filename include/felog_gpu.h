@@ -291,8 +291,8 @@ felog_status felog_walk_ceiling(felog_ctx *ctx, float *ms, uint64_t *tokens);
  * graph.hpp:531-575): next to the CSR, the library keeps every entry as 16
  * bytes {neighbour, data, the neighbour's first entry, its degree}, so a walk
  * step makes one dependent random read instead of two.  They are built by
- * load_graph / load_rmat for graphs of at most 2^31 CSR entries when the
- * device has room, and the walker and felog_walk_ceiling use them then.
+ * load_graph / load_rmat when the device has room for them (16 bytes per CSR
+ * entry), and the walker and felog_walk_ceiling use them then.
  * keep = 0 frees them (the walker reads the plain CSR from then on, until the
  * next graph load); bytes (may be NULL): their device size afterwards, 0 when
  * the walker reads the plain CSR. */

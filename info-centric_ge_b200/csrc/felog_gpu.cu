@@ -91,7 +91,7 @@ struct felog_ctx {
   uint64_t M = 0;
   DevBuf<uint64_t> row_ptr;
   DevBuf<uint2> adj;
-  DevBuf<uint4> wadj;  // walker entries (k_fuse_adj); empty above kFuseMaxEntries or without room
+  DevBuf<uint4> wadj;  // walker entries (k_fuse_adj); empty without room for them or once the caller frees them
   DevBuf<uint32_t> deg;
   std::vector<uint32_t> h_deg;
   DevBuf<float> alias_prob;
@@ -412,7 +412,6 @@ extern "C" const char *felog_last_error(const felog_ctx *c) { return c ? c->err.
 
 namespace {
 
-constexpr uint64_t kFuseMaxEntries = 1ull << 31;
 // host threads for init_model's per-word loops: a few, so that a busy shared
 // host does not hold a parallel region up on a descheduled thread
 #define FELOG_INIT_THREADS 8
@@ -467,10 +466,10 @@ felog_status build_csr(felog_ctx *c, const uint32_t *rec, uint64_t n, uint32_t v
   CK(cudaStreamSynchronize(c->stream), "load_graph");
   keys.release(); vals.release(); keys2.release(); vals2.release();
   c->cub_tmp.release();
-  // walker entries, while they take at most 32 GB (2^31 entries); without
-  // room for them the walk reads the plain CSR
+  // walker entries (16 B per entry, next to the 8-B CSR entry); without room
+  // for them the walk reads the plain CSR
   c->wadj.release();
-  if (m && m <= kFuseMaxEntries) {
+  if (m) {
     if (c->wadj.ensure(m) == cudaSuccess) {
       k_fuse_adj<<<grid_for(c, m, 256), 256, 0, c->stream>>>(c->row_ptr.p, c->adj.p, m, c->wadj.p);
       c->launches++;
