@@ -153,6 +153,7 @@ struct felog_ctx {
   DevBuf<uint64_t> pr_count, pr_off;  // pair stream: pairs per sentence, offsets
   DevBuf<int32_t> pr_rec;             // pair stream records
   int pair_minb = 0;                  // autotuned blocks per SM of the pair trainer (0: not tuned yet)
+  int tile_minb = 0;                  // autotuned blocks per SM of the tile kernels at -size 128 (0: not tuned yet)
   bool count_lost = false;            // BF16 pair trainer counts overwritten row updates (diagnostic)
   DevBuf<uint32_t> lost_ver0, lost_ver1;
   DevBuf<unsigned long long> lost_tot;
@@ -1994,25 +1995,82 @@ extern "C" felog_status felog_train_round(felog_ctx *c, uint32_t round, float al
       g.coarse = c->table_coarse.p;
       g.fm_table = make_fastmod((uint32_t)c->table_size);
     }
-#define FELOG_RT(D, K)                                                                             \
-  do {                                                                                             \
-    if (win) {                                                                                     \
-      if (bf) k_sgns_reuse_tile<D, K, RowsBF16, true><<<blocks, threads, 0, c->stream>>>(g);      \
-      else k_sgns_reuse_tile<D, K, RowsF32, true><<<blocks, threads, 0, c->stream>>>(g);          \
-    } else {                                                                                       \
-      if (bf) k_sgns_reuse_tile<D, K, RowsBF16><<<blocks, threads, 0, c->stream>>>(g);            \
-      else k_sgns_reuse_tile<D, K, RowsF32><<<blocks, threads, 0, c->stream>>>(g);                \
-    }                                                                                              \
+    // launch-shape autotuner: the first tiled round at -size 128 trains three
+    // slices of its sentences with register budgets for 4, 3 and 2 resident
+    // blocks per SM (real work, nothing repeated) and keeps the fastest per
+    // kept token
+    auto launch_tile = [&](const SgArgs &ga, int minb) {
+      const int K = c->o.negative, D = c->o.size;
+#define FELOG_RT(D_, K_, MB)                                                                              \
+  do {                                                                                                    \
+    if (win) {                                                                                            \
+      if (bf) k_sgns_reuse_tile<D_, K_, RowsBF16, true, MB><<<blocks, threads, 0, c->stream>>>(ga);      \
+      else k_sgns_reuse_tile<D_, K_, RowsF32, true, MB><<<blocks, threads, 0, c->stream>>>(ga);          \
+    } else {                                                                                              \
+      if (bf) k_sgns_reuse_tile<D_, K_, RowsBF16, false, MB><<<blocks, threads, 0, c->stream>>>(ga);     \
+      else k_sgns_reuse_tile<D_, K_, RowsF32, false, MB><<<blocks, threads, 0, c->stream>>>(ga);         \
+    }                                                                                                     \
   } while (0)
-    const int K = c->o.negative, D = c->o.size;
-    if (K == 5 && D == 64) FELOG_RT(64, 5);
-    else if (K == 5 && D == 128) FELOG_RT(128, 5);
-    else if (K == 5 && D == 256) FELOG_RT(256, 5);
-    else if (K == 7 && D == 64) FELOG_RT(64, 7);
-    else if (K == 7 && D == 128) FELOG_RT(128, 7);
-    else FELOG_RT(256, 7);
+      if (D == 128) {
+        if (K == 5) {
+          if (minb == 3) FELOG_RT(128, 5, 3);
+          else if (minb == 2) FELOG_RT(128, 5, 2);
+          else FELOG_RT(128, 5, 4);
+        } else {
+          if (minb == 3) FELOG_RT(128, 7, 3);
+          else if (minb == 2) FELOG_RT(128, 7, 2);
+          else FELOG_RT(128, 7, 4);
+        }
+      } else if (K == 5 && D == 64) FELOG_RT(64, 5, 4);
+      else if (K == 5 && D == 256) FELOG_RT(256, 5, 4);
+      else if (K == 7 && D == 64) FELOG_RT(64, 7, 4);
+      else FELOG_RT(256, 7, 4);
 #undef FELOG_RT
-    c->launches++;
+      c->launches++;
+    };
+    const uint64_t ns = g.n_sent;
+    constexpr int kTileCand = 3;
+    if (c->o.autotune && !c->o.deterministic && c->o.size == 128 && c->tile_minb == 0 &&
+        ns >= (uint64_t)kTileCand * blocks * (threads / 32)) {
+      const int cand[kTileCand] = {4, 3, 2};
+      cudaEvent_t ev[kTileCand + 1];
+      for (int i = 0; i <= kTileCand; i++) CK(cudaEventCreate(&ev[i]), "autotune");
+      uint64_t bound[kTileCand + 1];
+      for (int i = 0; i <= kTileCand; i++) bound[i] = ns * i / kTileCand;
+      for (int i = 0; i < kTileCand; i++) {
+        CK(cudaMemsetAsync(c->counters.p + 0, 0, 8, c->stream), "train");  // sentence claim counter
+        SgArgs gi = g;
+        gi.s_first = bound[i];
+        gi.n_sent = bound[i + 1] - bound[i];
+        CK(cudaEventRecord(ev[i], c->stream), "autotune");
+        launch_tile(gi, cand[i]);
+        CK(cudaGetLastError(), "train_round: launch");
+      }
+      CK(cudaEventRecord(ev[kTileCand], c->stream), "autotune");
+      uint64_t kept[kTileCand + 1];
+      for (int i = 0; i <= kTileCand; i++) RB(&kept[i], c->p_out_off.p + bound[i], 8, "autotune");
+      double best = 1e300;
+      int pick = 4;
+      char buf[256];
+      std::string rep = "tile blocks/SM:";
+      for (int i = 0; i < kTileCand; i++) {
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, ev[i], ev[i + 1]), "autotune");
+        const double per = ms / (double)std::max<uint64_t>(1, kept[i + 1] - kept[i]);
+        snprintf(buf, sizeof buf, " %d -> %.3f ns/token", cand[i], per * 1e6);
+        rep += buf;
+        if (per < best) {
+          best = per;
+          pick = cand[i];
+        }
+      }
+      snprintf(buf, sizeof buf, "; chose %d", pick);
+      c->tuning = rep + buf;
+      c->tile_minb = pick;
+      for (int i = 0; i <= kTileCand; i++) cudaEventDestroy(ev[i]);
+    } else {
+      launch_tile(g, c->tile_minb ? c->tile_minb : 4);
+    }
     CK(cudaGetLastError(), "train_round: launch");
   } else if (!c->o.cbow && c->o.size >= 64 && (c->o.negative == 5 || c->o.negative == 7)) {
     s = train_pairs(c, g, blocks, threads);

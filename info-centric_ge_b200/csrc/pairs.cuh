@@ -545,8 +545,10 @@ __global__ void __launch_bounds__(256, MINB)
 // the reference makes for its first context (:496-507); the LCG then jumps
 // past the K draws of every context of the center, so every center's window
 // is the reference's.  Lane q < K makes draw q; one table lookup per lane.
-template <int DIM, int NK, class P, bool WIN = false>
-__global__ void __launch_bounds__(256, 4) k_sgns_reuse_tile(SgArgs a) {
+// MINB: resident 256-thread blocks per SM the register budget is built for
+// (the autotuner picks among 4, 3 and 2 at DIM 128).
+template <int DIM, int NK, class P, bool WIN = false, int MINB = 4>
+__global__ void __launch_bounds__(256, MINB) k_sgns_reuse_tile(SgArgs a) {
   static_assert(DIM >= 64, "two or more values per lane");
   constexpr int H = DIM / 64;
   constexpr int NT = NK + 1;
@@ -557,8 +559,9 @@ __global__ void __launch_bounds__(256, 4) k_sgns_reuse_tile(SgArgs a) {
   LaneRows<DIM, P> rows;
   rows.init(a);
   unsigned long long my_pairs = 0;
-  unsigned long long s;
-  while (claim_sentence(a, s)) {
+  unsigned long long s_rel;
+  while (claim_sentence(a, s_rel)) {
+    const unsigned long long s = a.s_first + s_rel;
     const long long sb = (long long)a.sent_start[s], se = (long long)a.sent_start[s + 1];
     int neg[NK];
     unsigned long long nr = 0;  // WIN: the sentence's LCG, seeded by its index in the batch (word2vec.cu:446)

@@ -93,6 +93,7 @@ struct SgArgs {
   FastMod fm_table;
   const unsigned long long *jump_a, *jump_c;
   int *err;  // device error code (bounded waits that give up)
+  uint64_t s_first;  // tile kernels: the first sentence of this launch (claims count from it)
 };
 
 // ------------------------------------------------------------ row access
