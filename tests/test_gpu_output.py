@@ -91,7 +91,10 @@ def test_kmeans_objective_rises_to_a_fixed_point(precision):
     lab, obj = f.cluster(k, max_iter=200)
     assert lab.shape == (vs,) and lab.min() >= 0 and lab.max() < k
     assert len(obj) < 200, "did not converge in 200 passes"
-    assert np.all(np.diff(obj) >= -1e-9 * np.abs(obj[1:])), obj
+    # assignments compare FP32 dots, so a row whose two best centroids tie to
+    # FP32 rounding may move and lower the exact objective by a rounding error:
+    # the objective never falls by more than FP32 precision (2^-23 relative)
+    assert np.all(np.diff(obj) >= -2.0 ** -23 * np.abs(obj[1:])), obj
     # converged: the last pass changed nothing, so labels are a fixed point of both steps
     ref_obj, regret = _objective_and_fixed_point(rows, lab, k)
     assert regret <= 4e-5 * np.abs(rows).sum(axis=1).max()
