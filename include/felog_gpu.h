@@ -316,6 +316,15 @@ felog_status felog_common_neighbours(felog_ctx *ctx, const uint32_t *src, const 
 /* Vocabulary, unigram table and InitNet rows (word2vec.cu:834-902); also starts a new
  * training run: stop flags, visit counts and the budget records are cleared. */
 felog_status felog_init_model(felog_ctx *ctx);
+/* First slot of every word in the reference's unigram table (replaces the
+ * slot-by-slot loop of InitUnigramTable, word2vec.cu:674-694, with the same
+ * FP64 sums): counts[0..n) are the vocabulary's counts in vocabulary order
+ * (n <= 12.5 M words, the range where the table has the reference's 1e8
+ * slots); start[k] receives the first slot holding word k, so slot a holds
+ * the last word whose start is <= a (start values past the table's end mean
+ * the word gets no slot).  Host only: no device or context needed; init_model
+ * builds its table from these starts on the device. */
+felog_status felog_unigram_starts(const uint64_t *counts, uint64_t n, uint64_t *start);
 felog_status felog_vocab_info(felog_ctx *ctx, uint64_t *vocab_size, uint64_t *train_words);
 felog_status felog_get_vocab(felog_ctx *ctx, uint32_t *vocab_vertex, uint32_t *id2offset);
 /* alpha < 0: take the schedule value of round `round` */

@@ -1367,7 +1367,47 @@ __global__ void k_unigram_fill_starts(const uint64_t *__restrict__ start, uint64
     table[a] = (int32_t)lo;
   }
 }
+// First slot of every word in the reference's 1e8-slot unigram table (see
+// k_unigram_fill_starts): the words' shares cn^0.75 / total, their running
+// FP64 sums in the reference's order, the first slot past each sum, and the
+// prefix maximum that turns those into first slots.
+void unigram_starts(const long long *cn, long long size, uint64_t *start) {
+  const double power = 0.75, T = (double)kTableSize;
+  std::vector<double> w(size);
+  for (long long a = 0; a < size; a++) w[a] = (a > 0 && cn[a] == cn[a - 1]) ? w[a - 1] : pow((double)cn[a], power);
+  double twp = 0;
+  for (long long a = 0; a < size; a++) twp += w[a];
+  // D(k) in the reference's order, then firstA(k) per word (independent,
+  // on all host threads), then the prefix maximum
+  std::vector<double> dsum(size);
+  double d1 = w[0] / twp;
+  dsum[0] = d1;
+  for (long long k = 1; k < size; k++) dsum[k] = d1 += w[k] / twp;
+  std::vector<long long> fa(size);
+#pragma omp parallel for schedule(static) num_threads(FELOG_INIT_THREADS) if (size > 65536)
+  for (long long k = 0; k < size; k++) {
+    // firstA(k): the first slot a with a / T > D(k)
+    long long x = (long long)std::floor(dsum[k] * T);
+    if (x < 0) x = 0;
+    while (x > 0 && (double)(x - 1) / T > dsum[k]) x--;
+    while (!((double)x / T > dsum[k])) x++;
+    fa[k] = x;
+  }
+  long long run = 0;  // max_{j<k} (firstA(j) - j), or 0
+  for (long long k = 0; k < size; k++) {
+    start[k] = (uint64_t)(k + run);
+    run = std::max(run, fa[k] - k);
+  }
+}
 }  // namespace
+
+extern "C" felog_status felog_unigram_starts(const uint64_t *counts, uint64_t n, uint64_t *start) {
+  if (!counts || !start || n == 0 || n > (uint64_t)kRefTableMaxVocab) return FELOG_INVALID_ARG;
+  std::vector<long long> cn(n);
+  for (uint64_t i = 0; i < n; i++) cn[i] = (long long)counts[i];
+  unigram_starts(cn.data(), (long long)n, start);
+  return FELOG_OK;
+}
 
 extern "C" felog_status felog_init_model(felog_ctx *c) {
   if (!c) return FELOG_INVALID_ARG;
@@ -1420,33 +1460,8 @@ extern "C" felog_status felog_init_model(felog_ctx *c) {
     // unigram table (word2vec.cu:674-694): the reference's 1e8 slots and FP64
     // sums; the first slot of every word on the host (k_unigram_fill_starts
     // has the argument), the slots on the device
-    const double power = 0.75, T = (double)kTableSize;
-    std::vector<double> w(size);
-    for (long long a = 0; a < size; a++) w[a] = (a > 0 && cn[a] == cn[a - 1]) ? w[a - 1] : pow((double)cn[a], power);
-    double twp = 0;
-    for (long long a = 0; a < size; a++) twp += w[a];
-    // D(k) in the reference's order, then firstA(k) per word (independent,
-    // on all host threads), then the prefix maximum
-    std::vector<double> dsum(size);
-    double d1 = w[0] / twp;
-    dsum[0] = d1;
-    for (long long k = 1; k < size; k++) dsum[k] = d1 += w[k] / twp;
-    std::vector<long long> fa(size);
-#pragma omp parallel for schedule(static) num_threads(FELOG_INIT_THREADS) if (size > 65536)
-    for (long long k = 0; k < size; k++) {
-      // firstA(k): the first slot a with a / T > D(k)
-      long long x = (long long)std::floor(dsum[k] * T);
-      if (x < 0) x = 0;
-      while (x > 0 && (double)(x - 1) / T > dsum[k]) x--;
-      while (!((double)x / T > dsum[k])) x++;
-      fa[k] = x;
-    }
     std::vector<uint64_t> start(size);
-    long long run = 0;  // max_{j<k} (firstA(j) - j), or 0
-    for (long long k = 0; k < size; k++) {
-      start[k] = (uint64_t)(k + run);
-      run = std::max(run, fa[k] - k);
-    }
+    unigram_starts(cn.data(), size, start.data());
     c->table_size = kTableSize;
     CK(c->table.ensure(kTableSize), "init_model: unigram table");
     DevBuf<uint64_t> dstart;

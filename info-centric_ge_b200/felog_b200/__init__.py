@@ -159,6 +159,7 @@ def gpu_lib():
         L.felog_get_visit_freq.argtypes = [_P, _P]
         L.felog_walk_ceiling.argtypes = [_P, _P, _P]
         L.felog_walk_entries.argtypes = [_P, ctypes.c_int, _P]
+        L.felog_unigram_starts.argtypes = [_P, ctypes.c_uint64, _P]
         L.felog_pair_row_mix.argtypes = [_P, _P, _P, _P]
         L.felog_format_lf.argtypes = [_P, ctypes.c_uint64, _P, ctypes.c_uint64, _P]
         L.felog_common_neighbours.argtypes = [_P, _P, _P, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_int, _P, _P]
@@ -617,6 +618,17 @@ def synth_graph(seed, v_target, e_target, abcd=(0.57, 0.19, 0.19, 0.05), lognorm
 
 
 NOALLOC_MAX_ENTRIES = 1 << 22  # FELOG_NOALLOC_MAX_ENTRIES
+
+
+def unigram_starts(counts):
+    """First slot of every word in the reference's 1e8-slot unigram table
+    (felog_unigram_starts; host only)."""
+    c = np.ascontiguousarray(counts, dtype=np.uint64)
+    start = np.zeros(len(c), np.uint64)
+    st = gpu_lib().felog_unigram_starts(_addr(c), len(c), _addr(start))
+    if st != 0:
+        raise FelogError(st, "felog_unigram_starts failed (empty or more than 12.5 M words)")
+    return start
 
 
 def build_alias_noalloc(row_ptr_dev, weight_dev, v_num, e_num, prob_dev, alias_dev, stream=None):
