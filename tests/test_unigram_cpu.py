@@ -41,7 +41,16 @@ def zipf_counts():
     return np.sort(rng.zipf(1.7, size=2_000_000).clip(1, 10 ** 9))[::-1].astype(np.int64)
 
 
-@pytest.mark.parametrize("make", [c1_counts, lagging_counts, zipf_counts])
+def single_word():
+    return np.array([5], np.int64)
+
+
+def with_zero_counts():
+    # words of count 0 have no share; the reference's walk still passes through them one slot at a time
+    return np.array([1000, 500, 0, 0, 300, 0, 7, 1, 0], np.int64)
+
+
+@pytest.mark.parametrize("make", [c1_counts, lagging_counts, zipf_counts, single_word, with_zero_counts])
 def test_table_from_first_slots_equals_the_reference_loop(make):
     counts = make()
     start = fb.unigram_starts(counts)
